@@ -1,0 +1,235 @@
+"""dhara_b200 -- B200-native solver for Dhara's integrated surface-subsurface
+flow hot path (3D mixed-form Richards + 2D diffusive-wave overland).
+
+The compute lives in the CUDA library libdhara_b200.so behind the C ABI of
+include/dhara_gpu.h.  This module is a thin ctypes mirror of that ABI for
+Python callers (tests, benchmarks, notebooks); there is no CPU path: if the
+library cannot be loaded, every entry point raises.
+"""
+import ctypes as ct
+import os
+
+import numpy as np
+
+from . import _abi
+from ._abi import (FP64, MIXED, PICARD_PSI_RELATIVE, PICARD_THETA_RELATIVE, PICARD_PSI_ABSOLUTE,
+                   THETA_REFERENCE, THETA_FINAL, THETA_CONSERVATIVE, Params, Diagnostics, make_params)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdhara_b200.so")
+
+KERNELS = {"krylov": 0, "assemble": 1, "picard_check": 2, "epilogue": 3, "overland_solve": 4,
+           "overland_aux": 5, "prologue": 6}
+
+_lib = None
+
+
+class DharaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"dhara error {code} ({_abi.STATUS_NAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads libdhara_b200.so (building it first if only the sources exist)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    L = ct.CDLL(LIB_PATH)
+    P = ct.POINTER
+    vp, dp, i64p = ct.c_void_p, P(ct.c_double), P(ct.c_int64)
+    sig = {
+        "dhara_abi_version": (ct.c_int, []),
+        "dhara_last_error": (ct.c_char_p, []),
+        "dhara_default_params": (None, [P(Params), ct.c_int, ct.c_int, ct.c_int, ct.c_double,
+                                        ct.c_double, ct.c_double, ct.c_double]),
+        "dhara_create": (ct.c_int, [P(Params), ct.c_int, ct.c_int, P(vp)]),
+        "dhara_destroy": (ct.c_int, [vp]),
+        "dhara_upload": (ct.c_int, [vp, ct.c_int, ct.c_int, dp, ct.c_int64]),
+        "dhara_upload_int": (ct.c_int, [vp, ct.c_int, ct.c_int, P(ct.c_int32), ct.c_int64]),
+        "dhara_download": (ct.c_int, [vp, ct.c_int, ct.c_int, dp, ct.c_int64]),
+        "dhara_set_roots": (ct.c_int, [vp, ct.c_int, dp, ct.c_int]),
+        "dhara_set_rain_schedule": (ct.c_int, [vp, ct.c_int, dp, ct.c_int]),
+        "dhara_psi_from_theta": (ct.c_int, [vp]),
+        "dhara_prepare": (ct.c_int, [vp]),
+        "dhara_subsurface_step": (ct.c_int, [vp]),
+        "dhara_overland_step": (ct.c_int, [vp]),
+        "dhara_step": (ct.c_int, [vp, ct.c_int, ct.c_int]),
+        "dhara_synchronize": (ct.c_int, [vp]),
+        "dhara_get_diagnostics": (ct.c_int, [vp, ct.c_int, P(Diagnostics)]),
+        "dhara_get_stream": (ct.c_int, [vp, P(vp)]),
+        "dhara_set_kernel_timing": (ct.c_int, [vp, ct.c_int]),
+        "dhara_get_kernel_timing": (ct.c_int, [vp, ct.c_int, i64p, dp]),
+        "dhara_reset_kernel_timing": (ct.c_int, [vp]),
+        "dhara_get_launch_count": (ct.c_int, [vp, i64p]),
+        "dhara_get_krylov_traffic": (ct.c_int, [vp, dp, i64p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise DharaError(rc, lib().dhara_last_error().decode())
+
+
+def default_params(nx, ny, nz, dx, dy, dz, dt):
+    p = Params()
+    lib().dhara_default_params(ct.byref(p), nx, ny, nz, dx, dy, dz, dt)
+    return p
+
+
+def _dp(a):
+    return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+class Solver:
+    """One handle: ndomains independent domains advanced together on one GPU."""
+
+    def __init__(self, params, device=0):
+        plist = list(params) if isinstance(params, (list, tuple)) else [params]
+        arr = (Params * len(plist))(*plist)
+        h = ct.c_void_p()
+        _check(lib().dhara_create(arr, len(plist), device, ct.byref(h)))
+        self.h = h
+        self.params = plist
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dhara_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- data
+    def upload(self, name, arr, domain=0):
+        if name in _abi.FI:
+            a = np.ascontiguousarray(arr, dtype=np.int32)
+            _check(lib().dhara_upload_int(self.h, domain, _abi.FI[name],
+                                          a.ctypes.data_as(ct.POINTER(ct.c_int32)), a.size))
+        else:
+            a = np.ascontiguousarray(arr, dtype=np.float64)
+            _check(lib().dhara_upload(self.h, domain, _abi.F[name], _dp(a), a.size))
+
+    def download(self, name, domain=0):
+        out = np.empty(_abi.extent(self.params[domain], name), np.float64)
+        _check(lib().dhara_download(self.h, domain, _abi.F[name], _dp(out), out.size))
+        return out
+
+    def load(self, dom, domain=0, schedule=True):
+        """Uploads a dhara_b200.inputs.Domain (fields, BC types, rain schedule)."""
+        for k, v in dom.fields.items():
+            self.upload(k, v, domain)
+        for k, v in dom.int_fields.items():
+            if k == "procmap":
+                continue
+            self.upload(k, v, domain)
+        if schedule and len(dom.rain_mm):
+            self.set_rain_schedule(dom.rain_mm, domain)
+
+    def set_roots(self, rda, nproc, domain=0):
+        a = np.ascontiguousarray(rda, np.float64)
+        _check(lib().dhara_set_roots(self.h, domain, _dp(a), int(nproc)))
+
+    def set_rain_schedule(self, mm_per_step, domain=0):
+        a = np.ascontiguousarray(mm_per_step, np.float64)
+        _check(lib().dhara_set_rain_schedule(self.h, domain, _dp(a), a.size))
+
+    # -- the hot path
+    def psi_from_theta(self):
+        _check(lib().dhara_psi_from_theta(self.h))
+
+    def prepare(self):
+        _check(lib().dhara_prepare(self.h))
+
+    def subsurface_step(self):
+        _check(lib().dhara_subsurface_step(self.h))
+
+    def overland_step(self):
+        _check(lib().dhara_overland_step(self.h))
+
+    def step(self, nsteps=1, graph=False):
+        _check(lib().dhara_step(self.h, int(nsteps), 1 if graph else 0))
+
+    def synchronize(self):
+        _check(lib().dhara_synchronize(self.h))
+
+    def diagnostics(self, domain=0):
+        d = Diagnostics()
+        _check(lib().dhara_get_diagnostics(self.h, domain, ct.byref(d)))
+        return d.as_dict()
+
+    @property
+    def stream(self):
+        s = ct.c_void_p()
+        _check(lib().dhara_get_stream(self.h, ct.byref(s)))
+        return s.value or 0
+
+    # -- instrumentation
+    def set_kernel_timing(self, enable):
+        _check(lib().dhara_set_kernel_timing(self.h, 1 if enable else 0))
+
+    def kernel_timing(self, kernel):
+        n = ct.c_int64()
+        ms = ct.c_double()
+        _check(lib().dhara_get_kernel_timing(self.h, KERNELS.get(kernel, kernel), ct.byref(n),
+                                             ct.byref(ms)))
+        return n.value, ms.value
+
+    def reset_kernel_timing(self):
+        _check(lib().dhara_reset_kernel_timing(self.h))
+
+    def launch_count(self):
+        n = ct.c_int64()
+        _check(lib().dhara_get_launch_count(self.h, ct.byref(n)))
+        return n.value
+
+    def krylov_traffic(self):
+        b = ct.c_double()
+        n = ct.c_int64()
+        _check(lib().dhara_get_krylov_traffic(self.h, ct.byref(b), ct.byref(n)))
+        return b.value, n.value
+
+
+def run(domains, nsteps=None, graph=False, record=(), device=0):
+    """Runs one or several inputs.Domain objects together; returns per-domain
+    final states and diagnostics."""
+    doms = domains if isinstance(domains, (list, tuple)) else [domains]
+    s = Solver([d.params for d in doms], device=device)
+    for i, d in enumerate(doms):
+        s.load(d, i)
+    s.prepare()
+    n = nsteps if nsteps is not None else max(len(d.rain_mm) for d in doms)
+    rec = [{k: [] for k in record} for _ in doms]
+    if record:
+        for _ in range(n):
+            s.step(1, graph)
+            for i in range(len(doms)):
+                for k in record:
+                    rec[i][k].append(s.download(k, i))
+    else:
+        s.step(n, graph)
+    s.synchronize()
+    out = []
+    for i in range(len(doms)):
+        st = {k: s.download(k, i) for k in ("psi", "theta", "ponding", "waterelev", "K")}
+        out.append((st, s.diagnostics(i), rec[i]))
+    s.close()
+    return out if isinstance(domains, (list, tuple)) else out[0]

@@ -1,0 +1,792 @@
+// api.cu -- the C ABI of include/dhara_gpu.h: handle lifetime, device memory
+// layout, uploads/downloads, and the launch sequence of one coupled step.
+//
+// One time step for every domain of a handle (the reference's
+// SubsurfaceFlowModel then OverlandFlowModel, src/device.cu:450-458) is a
+// fixed launch sequence with no host synchronisation:
+//   k_prologue; [k_assemble, k_krylov (persistent), k_picard_check] x maxiter;
+//   k_epilogue; k_olf_setup, k_olf_solve (persistent), k_olf_finish
+// Domains whose Picard loop has converged skip the remaining iterations on the
+// device, so the sequence can be captured once into a CUDA graph and replayed.
+#include "internal.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err = "no error";
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(DHARA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
+    } while (0)
+
+enum { KT_KRYLOV = 0, KT_ASSEMBLE, KT_CHECK, KT_EPILOGUE, KT_OLF_SOLVE, KT_OLF_AUX, KT_PROLOGUE, KT_N };
+
+}  // namespace
+
+struct dhara_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int ndom = 0;
+    int mixed = 0;
+    int nz_max = 1;
+    int maxiter_picard = 1;
+    std::vector<dhara_params> params;
+    std::vector<DomainDesc> hdom;
+    std::vector<TileDesc> htiles;
+    long long Ntot = 0, Ctot = 0, WEtot = 0, SNtot = 0;
+    DevPtrs P{};
+    LaunchCfg L{};
+    std::vector<void *> allocs;
+    double *scratch = nullptr;
+    DomainDesc *d_dom = nullptr;
+    std::vector<int> nproc;
+    std::vector<std::vector<double>> roots;
+    std::vector<std::vector<double>> sched;
+    std::vector<unsigned> uploaded;  // bitmask per domain
+    bool prepared = false;
+    // graph replay
+    cudaGraphExec_t graph_exec = nullptr;
+    bool graph_failed = false;
+    // timing
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[KT_N];
+    std::vector<cudaEvent_t> event_pool;
+    double total_ms[KT_N] = {};
+    long long launches[KT_N] = {};
+    long long launch_count = 0;
+};
+
+namespace {
+
+enum { UP_PSI = 1, UP_THETA = 2, UP_KSAT = 4, UP_ZTOPO = 8 };
+
+template <typename T>
+int dalloc(dhara_handle *h, T **p, size_t count) {
+    void *q = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DHARA_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T),
+                    cudaGetErrorString(e));
+    }
+    h->allocs.push_back(q);
+    *p = (T *)q;
+    return DHARA_OK;
+}
+
+int dalloc_void(dhara_handle *h, void **p, size_t bytes) {
+    char *q = nullptr;
+    int rc = dalloc(h, &q, bytes);
+    *p = q;
+    return rc;
+}
+
+int validate(const dhara_params &p, int d) {
+    if (p.struct_size != (int)sizeof(dhara_params))
+        return fail(DHARA_ERR_INVALID, "domain %d: struct_size %d != sizeof(dhara_params) %d", d,
+                    p.struct_size, (int)sizeof(dhara_params));
+    if (p.nx < 1 || p.ny < 1 || p.nz < 1)
+        return fail(DHARA_ERR_INVALID, "domain %d: grid %dx%dx%d must be positive", d, p.nx, p.ny, p.nz);
+    if (p.nz > NZ_MAX)
+        return fail(DHARA_ERR_UNSUPPORTED, "domain %d: nz=%d exceeds the column limit %d", d, p.nz, NZ_MAX);
+    if (!(p.dx > 0) || !(p.dy > 0) || !(p.dz > 0) || !(p.dt > 0))
+        return fail(DHARA_ERR_INVALID, "domain %d: dx, dy, dz, dt must be > 0", d);
+    if (!(p.theta_s > p.theta_r) || !(p.n > 1.0) || !(p.alpha > 0) || !(p.porosity > 0) || !(p.Ss >= 0))
+        return fail(DHARA_ERR_INVALID, "domain %d: invalid van Genuchten parameters", d);
+    if (p.picard_maxiter < 1 || p.krylov_maxiter < 1 || p.overland_maxiter < 0)
+        return fail(DHARA_ERR_INVALID, "domain %d: iteration caps must be positive", d);
+    if (!(p.am >= 0.0 && p.am < 1.0))
+        return fail(DHARA_ERR_INVALID, "domain %d: am must be in [0, 1)", d);
+    if (p.picard_rule < 0 || p.picard_rule > 2 || p.theta_update < 0 || p.theta_update > 2)
+        return fail(DHARA_ERR_INVALID, "domain %d: unknown picard_rule / theta_update", d);
+    if (p.precision != DHARA_FP64 && p.precision != DHARA_MIXED)
+        return fail(DHARA_ERR_INVALID, "domain %d: unknown precision %d", d, p.precision);
+    if (!(p.krylov_tol > 0) || !(p.overland_tol > 0) || !(p.picard_tol > 0))
+        return fail(DHARA_ERR_INVALID, "domain %d: tolerances must be > 0", d);
+    return DHARA_OK;
+}
+
+int set_dev(dhara_handle *h) {
+    CK(cudaSetDevice(h->device));
+    return DHARA_OK;
+}
+
+cudaEvent_t get_event(dhara_handle *h) {
+    if (!h->event_pool.empty()) {
+        cudaEvent_t e = h->event_pool.back();
+        h->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct Timed {
+    dhara_handle *h;
+    int kind;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timed(dhara_handle *hh, int k) : h(hh), kind(k) {
+        h->launch_count += 1;
+        h->launches[kind] += 1;
+        if (h->timing) {
+            a = get_event(h);
+            b = get_event(h);
+            cudaEventRecord(a, h->stream);
+        }
+    }
+    ~Timed() {
+        if (h->timing) {
+            cudaEventRecord(b, h->stream);
+            h->pending[kind].push_back({a, b});
+        }
+    }
+};
+
+void collect_timing(dhara_handle *h) {
+    for (int k = 0; k < KT_N; ++k) {
+        for (auto &pr : h->pending[k]) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) h->total_ms[k] += ms;
+            h->event_pool.push_back(pr.first);
+            h->event_pool.push_back(pr.second);
+        }
+        h->pending[k].clear();
+    }
+}
+
+#define LAUNCH(kind, call)                                                                     \
+    do {                                                                                       \
+        Timed t_(h, kind);                                                                     \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(DHARA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));       \
+    } while (0)
+
+int enqueue_subsurface(dhara_handle *h) {
+    const DevPtrs &P = h->P;
+    cudaStream_t s = h->stream;
+    LAUNCH(KT_PROLOGUE, launch_prologue(P, s));
+    for (int m = 0; m < h->maxiter_picard; ++m) {
+        LAUNCH(KT_ASSEMBLE, launch_assemble(P, h->L, s));
+        LAUNCH(KT_KRYLOV, launch_krylov(P, h->L, s));
+        LAUNCH(KT_CHECK, launch_picard_check(P, s));
+    }
+    LAUNCH(KT_EPILOGUE, launch_epilogue(P, h->L, s));
+    return DHARA_OK;
+}
+
+int enqueue_overland(dhara_handle *h) {
+    const DevPtrs &P = h->P;
+    cudaStream_t s = h->stream;
+    LAUNCH(KT_OLF_AUX, launch_overland_setup(P, h->Ctot, s));
+    LAUNCH(KT_OLF_SOLVE, launch_overland_solve(P, h->L, h->Ctot, s));
+    LAUNCH(KT_OLF_AUX, launch_overland_finish(P, h->Ctot, s));
+    return DHARA_OK;
+}
+
+int check_device_error(dhara_handle *h) {
+    GridBarrier gb;
+    CK(cudaMemcpyAsync(&gb, h->P.barrier, sizeof(gb), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (gb.error)
+        return fail(DHARA_ERR_TIMEOUT, "a persistent kernel's grid barrier timed out; results are invalid");
+    return DHARA_OK;
+}
+
+struct FieldLoc {
+    void *ptr;
+    long long count;
+    size_t elt;
+    bool is_int;
+    bool computed;  // download evaluates the closure
+    int which;
+};
+
+int locate(dhara_handle *h, int dom, int field, FieldLoc *out) {
+    if (dom < 0 || dom >= h->ndom) return fail(DHARA_ERR_INVALID, "domain %d out of range", dom);
+    const DomainDesc &D = h->hdom[dom];
+    const long long N = (long long)D.nx * D.ny * D.nz, C = (long long)D.nx * D.ny;
+    const long long WE = (long long)D.nz * D.ny, SN = (long long)D.nz * D.nx;
+    DevPtrs &P = h->P;
+    FieldLoc f{nullptr, 0, sizeof(double), false, false, 0};
+    switch (field) {
+        case DHARA_F_PSI: f.ptr = P.psin + D.off3; f.count = N; break;
+        case DHARA_F_THETA: f.ptr = P.thetan + D.off3; f.count = N; break;
+        case DHARA_F_KSAT: f.ptr = P.ksat + D.off3; f.count = N; break;
+        case DHARA_F_ALPHA:
+            if (!P.alpha && dalloc(h, &P.alpha, (size_t)h->Ntot)) return DHARA_ERR_NOMEM;
+            f.ptr = P.alpha + D.off3; f.count = N; break;
+        case DHARA_F_NVG:
+            if (!P.nvg && dalloc(h, &P.nvg, (size_t)h->Ntot)) return DHARA_ERR_NOMEM;
+            f.ptr = P.nvg + D.off3; f.count = N; break;
+        case DHARA_F_K: f.count = N; f.computed = true; f.which = 1; break;
+        case DHARA_F_C: f.count = N; f.computed = true; f.which = 2; break;
+        case DHARA_F_THETA_NEW: f.count = N; f.computed = true; f.which = 0; break;
+        case DHARA_F_ZTOPO: f.ptr = P.ztopo + D.off2; f.count = C; break;
+        case DHARA_F_MANN: f.ptr = P.mann + D.off2; f.count = C; break;
+        case DHARA_F_WATERDEPTH: f.ptr = P.h + D.off2; f.count = C; break;
+        case DHARA_F_WATERELEV: f.ptr = P.H + D.off2; f.count = C; break;
+        case DHARA_F_PONDING: f.ptr = P.ph + D.off2; f.count = C; break;
+        case DHARA_F_PPT: f.ptr = P.ppt + D.off2; f.count = C; break;
+        case DHARA_F_ESOIL: f.ptr = P.esoil + D.off2; f.count = C; break;
+        case DHARA_F_TR: f.ptr = P.tr + D.off2; f.count = C; break;
+        case DHARA_F_HPOTEN: f.ptr = P.hpoten + D.off2; f.count = C; break;
+        case DHARA_F_QTOP: f.ptr = P.qtop + D.off2; f.count = C; break;
+        case DHARA_F_BCQB: f.ptr = P.bcqb + D.off2; f.count = C; break;
+        case DHARA_F_BCQW: f.ptr = P.bcqw + D.offWE; f.count = WE; break;
+        case DHARA_F_BCQE: f.ptr = P.bcqe + D.offWE; f.count = WE; break;
+        case DHARA_F_BCQS: f.ptr = P.bcqs + D.offSN; f.count = SN; break;
+        case DHARA_F_BCQN: f.ptr = P.bcqn + D.offSN; f.count = SN; break;
+        case DHARA_F_BCPSIW: case DHARA_F_BCPSIE: f.count = WE; break;
+        case DHARA_F_BCPSIS: case DHARA_F_BCPSIN: f.count = SN; break;
+        case DHARA_F_BCPSIB: f.count = C; break;
+        case DHARA_FI_BCW: case DHARA_FI_BCE: f.count = WE; f.is_int = true; f.elt = 4; break;
+        case DHARA_FI_BCS: case DHARA_FI_BCN: f.count = SN; f.is_int = true; f.elt = 4; break;
+        case DHARA_FI_BCB: case DHARA_FI_BCT: f.count = C; f.is_int = true; f.elt = 4; break;
+        case DHARA_FI_PROCMAP: f.ptr = P.procmap + D.off2; f.count = C; f.is_int = true; f.elt = 4; break;
+        default: return fail(DHARA_ERR_INVALID, "unknown field id %d", field);
+    }
+    *out = f;
+    return DHARA_OK;
+}
+
+int upload_dom_desc(dhara_handle *h) {
+    CK(cudaMemcpyAsync(h->d_dom, h->hdom.data(), sizeof(DomainDesc) * h->ndom, cudaMemcpyHostToDevice,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return DHARA_OK;
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+const char *dhara_last_error(void) { return g_err.c_str(); }
+int dhara_abi_version(void) { return DHARA_ABI_VERSION; }
+
+void dhara_default_params(dhara_params *p, int nx, int ny, int nz, double dx, double dy, double dz,
+                          double dt) {
+    std::memset(p, 0, sizeof(*p));
+    p->struct_size = (int32_t)sizeof(dhara_params);
+    p->nx = nx; p->ny = ny; p->nz = nz;
+    p->dx = dx; p->dy = dy; p->dz = dz; p->dt = dt;
+    // include/devconst.h:13-31, alpha 0.02 /cm = 2.0 /m
+    p->alpha = 2.0; p->n = 1.8; p->theta_s = 0.45; p->theta_r = 0.1; p->porosity = 0.45; p->Ss = 5e-4;
+    p->airdry = -5.0; p->psimin = 5e-3; p->am = 0.0;
+    p->delta = 1e-7; p->hmin = 1e-5; p->hcri = 0.0; p->K0 = 1e-5;
+    p->sec_p_mm2dt_p_m = dt / 1000.0;
+    // MAXIMUM_ITERATIONS, PICARD_METHOD, TOLERANCE_PRESSURE (examples/1-EBI/ebi.cfg)
+    p->picard_maxiter = 10; p->picard_rule = DHARA_PICARD_PSI_RELATIVE; p->picard_tol = 1e-8;
+    // cusp::monitor(rhs, 100, 1e-8) and (rhs2d, 100, 1e-9): src/subsurface.cu:750, overland.cu:410
+    p->krylov_maxiter = 100; p->krylov_tol = 1e-8; p->theta_update = DHARA_THETA_REFERENCE;
+    p->overland_maxiter = 100; p->overland_tol = 1e-9; p->precision = DHARA_FP64;
+    p->inner_tol = 1e-4; p->inner_maxiter = 60;
+}
+
+int dhara_create(const dhara_params *params, int ndomains, int device, dhara_handle **out) {
+    if (!out) return fail(DHARA_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!params || ndomains < 1) return fail(DHARA_ERR_INVALID, "need at least one domain");
+    for (int d = 0; d < ndomains; ++d) {
+        int rc = validate(params[d], d);
+        if (rc) return rc;
+        if (params[d].precision != params[0].precision)
+            return fail(DHARA_ERR_INVALID, "all domains of a handle must share one precision");
+    }
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (device < 0) CK(cudaGetDevice(&device));
+    if (device >= ndev) return fail(DHARA_ERR_INVALID, "device %d of %d", device, ndev);
+    dhara_handle *h = new dhara_handle();
+    h->device = device;
+    h->ndom = ndomains;
+    h->params.assign(params, params + ndomains);
+    h->mixed = params[0].precision == DHARA_MIXED;
+    auto bail = [&](int rc) {
+        dhara_destroy(h);
+        return rc;
+    };
+    if (set_dev(h)) return bail(DHARA_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(DHARA_ERR_CUDA, "cudaStreamCreate failed"));
+
+    // domains, offsets and tiles
+    h->hdom.resize(ndomains);
+    for (int d = 0; d < ndomains; ++d) {
+        const dhara_params &p = params[d];
+        DomainDesc &D = h->hdom[d];
+        std::memset(&D, 0, sizeof(D));
+        D.nx = p.nx; D.ny = p.ny; D.nz = p.nz;
+        D.picard_rule = p.picard_rule; D.theta_update = p.theta_update;
+        D.picard_maxiter = p.picard_maxiter; D.krylov_maxiter = p.krylov_maxiter;
+        D.overland_maxiter = p.overland_maxiter;
+        D.inner_maxiter = h->mixed ? (p.inner_maxiter > 0 ? p.inner_maxiter : p.krylov_maxiter) : p.krylov_maxiter;
+        D.off3 = h->Ntot; D.off2 = h->Ctot; D.offWE = h->WEtot; D.offSN = h->SNtot;
+        h->Ntot += (long long)p.nx * p.ny * p.nz;
+        h->Ctot += (long long)p.nx * p.ny;
+        h->WEtot += (long long)p.nz * p.ny;
+        h->SNtot += (long long)p.nz * p.nx;
+        D.dx = p.dx; D.dy = p.dy; D.dz = p.dz; D.dt = p.dt;
+        D.alpha = p.alpha; D.n = p.n; D.theta_s = p.theta_s; D.theta_r = p.theta_r;
+        D.porosity = p.porosity; D.Ss = p.Ss; D.am = p.am;
+        D.delta = p.delta; D.hmin = p.hmin; D.K0 = p.K0; D.sec = p.sec_p_mm2dt_p_m;
+        D.picard_tol = p.picard_tol; D.krylov_tol = p.krylov_tol;
+        D.inner_tol = h->mixed ? (p.inner_tol > 0 ? p.inner_tol : 1e-4) : 0.0;
+        D.overland_tol = p.overland_tol;
+        D.closure_fp32 = (h->mixed && p.closure_fp32) ? 1 : 0;
+        D.tile_begin = (int)h->htiles.size();
+        for (int y0 = 0; y0 < p.ny; y0 += TILE_Y)
+            for (int x0 = 0; x0 < p.nx; x0 += TILE_X) h->htiles.push_back({d, x0, y0, 0});
+        D.tile_end = (int)h->htiles.size();
+        if (p.nz > h->nz_max) h->nz_max = p.nz;
+        if (p.picard_maxiter > h->maxiter_picard) h->maxiter_picard = p.picard_maxiter;
+    }
+    h->nproc.assign(ndomains, 1);
+    h->roots.assign(ndomains, std::vector<double>());
+    h->sched.assign(ndomains, std::vector<double>());
+    h->uploaded.assign(ndomains, 0u);
+
+    DevPtrs &P = h->P;
+    const size_t N = (size_t)h->Ntot, C = (size_t)h->Ctot;
+    const size_t sT = h->mixed ? sizeof(float) : sizeof(double);
+    int rc = 0;
+    rc |= dalloc(h, &h->d_dom, ndomains);
+    TileDesc *d_tiles = nullptr;
+    rc |= dalloc(h, &d_tiles, h->htiles.size());
+    for (double **q : {&P.psin, &P.thetan, &P.psim, &P.x, &P.b, &P.ksat}) rc |= dalloc(h, q, N);
+    for (void **q : {&P.K, &P.D, &P.r, &P.p0, &P.p1, &P.z, &P.d}) rc |= dalloc_void(h, q, N * sT);
+    if (h->mixed) {
+        rc |= dalloc(h, &P.K64, N);
+        rc |= dalloc(h, &P.D64, N);
+    } else {
+        P.K64 = (double *)P.K;
+        P.D64 = (double *)P.D;
+    }
+    for (double **q : {&P.ztopo, &P.mann, &P.h, &P.H, &P.ph, &P.ppt, &P.esoil, &P.tr, &P.hpoten, &P.qtop,
+                       &P.ktop, &P.bcqb, &P.olf_b, &P.olf_r, &P.olf_p0, &P.olf_p1, &P.olf_z})
+        rc |= dalloc(h, q, C);
+    rc |= dalloc(h, &P.olf_k, 4 * C);
+    rc |= dalloc(h, &P.bcqw, (size_t)h->WEtot);
+    rc |= dalloc(h, &P.bcqe, (size_t)h->WEtot);
+    rc |= dalloc(h, &P.bcqs, (size_t)h->SNtot);
+    rc |= dalloc(h, &P.bcqn, (size_t)h->SNtot);
+    rc |= dalloc(h, &P.procmap, C);
+    P.nproc_max = 1;
+    P.rda_stride = h->nz_max;
+    rc |= dalloc(h, &P.rda, (size_t)ndomains * P.rda_stride);
+    rc |= dalloc(h, &P.kctrl, ndomains);
+    rc |= dalloc(h, &P.pctrl, ndomains);
+    rc |= dalloc(h, &P.octrl, ndomains);
+    rc |= dalloc(h, &P.diag, ndomains);
+    rc |= dalloc(h, &P.gctrl, 1);
+    rc |= dalloc(h, &P.barrier, 1);
+    rc |= dalloc(h, &P.partials, h->htiles.size() * NPART);
+    rc |= dalloc(h, &P.arrive, (size_t)ndomains * 4);
+    rc |= dalloc(h, &P.step_acc, (size_t)ndomains * 16);
+    if (rc) return bail(DHARA_ERR_NOMEM);
+    P.dom = h->d_dom;
+    P.tiles = d_tiles;
+    P.ntiles = (int)h->htiles.size();
+    P.ndom = ndomains;
+    P.alpha = P.nvg = nullptr;
+    P.rain_sched = nullptr;
+
+    // zero everything so unset inputs are defined (fluxes 0, procmap 0, roots 0)
+    for (void *q : h->allocs) {
+        (void)q;
+    }
+    auto zero = [&](void *p, size_t bytes) { return cudaMemsetAsync(p, 0, bytes, h->stream); };
+    cudaError_t e = cudaSuccess;
+    for (double *q : {P.psin, P.thetan, P.psim, P.x, P.b, P.ksat}) e = e ? e : zero(q, N * 8);
+    for (void *q : {P.K, P.D, P.r, P.p0, P.p1, P.z, P.d}) e = e ? e : zero(q, N * sT);
+    for (double *q : {P.K64, P.D64}) e = e ? e : zero(q, N * 8);
+    for (double *q : {P.ztopo, P.mann, P.h, P.H, P.ph, P.ppt, P.esoil, P.tr, P.hpoten, P.qtop, P.ktop, P.bcqb,
+                      P.olf_b, P.olf_r, P.olf_p0, P.olf_p1, P.olf_z})
+        e = e ? e : zero(q, C * 8);
+    e = e ? e : zero(P.olf_k, 4 * C * 8);
+    e = e ? e : zero(P.bcqw, (size_t)h->WEtot * 8);
+    e = e ? e : zero(P.bcqe, (size_t)h->WEtot * 8);
+    e = e ? e : zero(P.bcqs, (size_t)h->SNtot * 8);
+    e = e ? e : zero(P.bcqn, (size_t)h->SNtot * 8);
+    e = e ? e : zero(P.procmap, C * 4);
+    e = e ? e : zero(P.rda, (size_t)ndomains * P.rda_stride * 8);
+    e = e ? e : zero(P.kctrl, ndomains * sizeof(KrylovCtrl));
+    e = e ? e : zero(P.pctrl, ndomains * sizeof(PicardCtrl));
+    e = e ? e : zero(P.octrl, ndomains * sizeof(OverlandCtrl));
+    e = e ? e : zero(P.diag, ndomains * sizeof(DevDiag));
+    e = e ? e : zero(P.gctrl, sizeof(GlobalCtrl));
+    e = e ? e : zero(P.barrier, sizeof(GridBarrier));
+    e = e ? e : zero(P.partials, h->htiles.size() * NPART * 8);
+    e = e ? e : zero(P.arrive, (size_t)ndomains * 4 * 4);
+    e = e ? e : zero(P.step_acc, (size_t)ndomains * 16 * 8);
+    if (e != cudaSuccess) return bail(fail(DHARA_ERR_CUDA, "initialising device memory: %s", cudaGetErrorString(e)));
+    if (cudaMemcpyAsync(d_tiles, h->htiles.data(), sizeof(TileDesc) * h->htiles.size(), cudaMemcpyHostToDevice,
+                        h->stream) != cudaSuccess)
+        return bail(fail(DHARA_ERR_CUDA, "tile upload failed"));
+    if (upload_dom_desc(h)) return bail(DHARA_ERR_CUDA);
+
+    h->L.nz_max = h->nz_max;
+    h->L.mixed = h->mixed;
+    e = configure_3d(h->L, device, P.ntiles);
+    if (e == cudaSuccess) e = configure_2d(h->L, device);
+    if (e != cudaSuccess) return bail(fail(DHARA_ERR_CUDA, "kernel configuration: %s", cudaGetErrorString(e)));
+    *out = h;
+    return DHARA_OK;
+}
+
+int dhara_destroy(dhara_handle *h) {
+    if (!h) return DHARA_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    for (int k = 0; k < KT_N; ++k)
+        for (auto &pr : h->pending[k]) {
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
+    for (cudaEvent_t ev : h->event_pool) cudaEventDestroy(ev);
+    for (void *q : h->allocs) cudaFree(q);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return DHARA_OK;
+}
+
+int dhara_upload(dhara_handle *h, int domain, int field, const double *src, int64_t count) {
+    if (!h || !src) return fail(DHARA_ERR_INVALID, "NULL handle or source");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    FieldLoc f;
+    int rc = locate(h, domain, field, &f);
+    if (rc) return rc;
+    if (f.is_int) return fail(DHARA_ERR_INVALID, "field %d is an int32 field", field);
+    if (f.computed) return fail(DHARA_ERR_INVALID, "field %d is output-only", field);
+    if (count != f.count) return fail(DHARA_ERR_INVALID, "field %d expects %lld values, got %lld", field,
+                                      (long long)f.count, (long long)count);
+    for (int64_t i = 0; i < count; ++i)
+        if (!std::isfinite(src[i]))
+            return fail(DHARA_ERR_NONFINITE, "field %d value %lld is not finite", field, (long long)i);
+    if (!f.ptr) return DHARA_OK;  // Dirichlet values: only meaningful with Dirichlet faces
+    CK(cudaMemcpyAsync(f.ptr, src, count * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (field == DHARA_F_ALPHA || field == DHARA_F_NVG) {
+        if (field == DHARA_F_ALPHA) h->hdom[domain].has_alpha = 1;
+        else h->hdom[domain].has_n = 1;
+        if (upload_dom_desc(h)) return DHARA_ERR_CUDA;
+    }
+    if (field == DHARA_F_PSI) h->uploaded[domain] |= UP_PSI;
+    if (field == DHARA_F_THETA) h->uploaded[domain] |= UP_THETA;
+    if (field == DHARA_F_KSAT) h->uploaded[domain] |= UP_KSAT;
+    if (field == DHARA_F_ZTOPO) h->uploaded[domain] |= UP_ZTOPO;
+    return DHARA_OK;
+}
+
+int dhara_upload_int(dhara_handle *h, int domain, int field, const int32_t *src, int64_t count) {
+    if (!h || !src) return fail(DHARA_ERR_INVALID, "NULL handle or source");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    FieldLoc f;
+    int rc = locate(h, domain, field, &f);
+    if (rc) return rc;
+    if (!f.is_int) return fail(DHARA_ERR_INVALID, "field %d is a double field", field);
+    if (count != f.count) return fail(DHARA_ERR_INVALID, "field %d expects %lld values, got %lld", field,
+                                      (long long)f.count, (long long)count);
+    if (field == DHARA_FI_PROCMAP) {
+        for (int64_t i = 0; i < count; ++i)
+            if (src[i] < 0 || src[i] >= h->nproc[domain])
+                return fail(DHARA_ERR_INVALID, "procmap[%lld]=%d outside [0, %d) (call dhara_set_roots first)",
+                            (long long)i, src[i], h->nproc[domain]);
+        CK(cudaMemcpyAsync(f.ptr, src, count * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return DHARA_OK;
+    }
+    if (field == DHARA_FI_BCT) return DHARA_OK;  // the top is always a flux face (src/global.cu:236-251)
+    for (int64_t i = 0; i < count; ++i)
+        if (src[i] == 0)
+            return fail(DHARA_ERR_UNSUPPORTED,
+                        "Dirichlet (type 0) side/bottom faces are not implemented on the GPU path");
+    return DHARA_OK;
+}
+
+int dhara_download(dhara_handle *h, int domain, int field, double *dst, int64_t count) {
+    if (!h || !dst) return fail(DHARA_ERR_INVALID, "NULL handle or destination");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    FieldLoc f;
+    int rc = locate(h, domain, field, &f);
+    if (rc) return rc;
+    if (f.is_int) return fail(DHARA_ERR_INVALID, "field %d is an int32 field", field);
+    if (count != f.count) return fail(DHARA_ERR_INVALID, "field %d holds %lld values, asked %lld", field,
+                                      (long long)f.count, (long long)count);
+    const DomainDesc &D = h->hdom[domain];
+    if (f.computed) {
+        if (!h->scratch && dalloc(h, &h->scratch, (size_t)h->Ntot)) return DHARA_ERR_NOMEM;
+        CK(launch_eval_fields(h->P, f.which, h->scratch, h->stream));
+        f.ptr = h->scratch + D.off3;
+    }
+    if (!f.ptr) return fail(DHARA_ERR_INVALID, "field %d is not stored on the GPU path", field);
+    CK(cudaMemcpyAsync(dst, f.ptr, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return DHARA_OK;
+}
+
+int dhara_set_roots(dhara_handle *h, int domain, const double *rda, int nproc) {
+    if (!h || !rda || nproc < 1) return fail(DHARA_ERR_INVALID, "bad arguments");
+    if (domain < 0 || domain >= h->ndom) return fail(DHARA_ERR_INVALID, "domain out of range");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    const int nz = h->hdom[domain].nz;
+    h->nproc[domain] = nproc;
+    h->roots[domain].assign(rda, rda + (size_t)nproc * nz);
+    int nproc_max = 1;
+    for (int n : h->nproc) nproc_max = n > nproc_max ? n : nproc_max;
+    const int stride = nproc_max * h->nz_max;
+    std::vector<double> all((size_t)h->ndom * stride, 0.0);
+    for (int d = 0; d < h->ndom; ++d)
+        for (size_t q = 0; q < h->roots[d].size(); ++q) all[(size_t)d * stride + q] = h->roots[d][q];
+    if (stride != h->P.rda_stride) {
+        double *p = nullptr;
+        if (dalloc(h, &p, all.size())) return DHARA_ERR_NOMEM;
+        h->P.rda = p;
+        h->P.rda_stride = stride;
+        h->P.nproc_max = nproc_max;
+        if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+    }
+    CK(cudaMemcpyAsync(h->P.rda, all.data(), all.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return DHARA_OK;
+}
+
+int dhara_set_rain_schedule(dhara_handle *h, int domain, const double *mm, int nsteps) {
+    if (!h || (nsteps > 0 && !mm) || nsteps < 0) return fail(DHARA_ERR_INVALID, "bad arguments");
+    if (domain < 0 || domain >= h->ndom) return fail(DHARA_ERR_INVALID, "domain out of range");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    h->sched[domain].assign(mm, mm + nsteps);
+    std::vector<double> all;
+    for (int d = 0; d < h->ndom; ++d) {
+        h->hdom[d].sched_off = (long long)all.size();
+        h->hdom[d].sched_len = (int)h->sched[d].size();
+        all.insert(all.end(), h->sched[d].begin(), h->sched[d].end());
+    }
+    double *p = nullptr;
+    if (dalloc(h, &p, all.size())) return DHARA_ERR_NOMEM;
+    if (!all.empty())
+        CK(cudaMemcpyAsync(p, all.data(), all.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    h->P.rain_sched = p;
+    if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+    return upload_dom_desc(h);
+}
+
+int dhara_psi_from_theta(dhara_handle *h) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    for (int d = 0; d < h->ndom; ++d)
+        if (!(h->uploaded[d] & UP_THETA)) return fail(DHARA_ERR_STATE, "domain %d: theta not uploaded", d);
+    CK(launch_psi_from_theta(h->P, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int d = 0; d < h->ndom; ++d) h->uploaded[d] |= UP_PSI;
+    return DHARA_OK;
+}
+
+int dhara_prepare(dhara_handle *h) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    for (int d = 0; d < h->ndom; ++d) {
+        const unsigned need = UP_PSI | UP_KSAT | UP_ZTOPO;
+        if ((h->uploaded[d] & need) != need)
+            return fail(DHARA_ERR_STATE, "domain %d: psi (or theta + dhara_psi_from_theta), ksat and ztopo "
+                                         "must be uploaded before dhara_prepare", d);
+    }
+    const DevPtrs &P = h->P;
+    CK(cudaMemsetAsync(P.pctrl, 0, h->ndom * sizeof(PicardCtrl), h->stream));
+    CK(cudaMemsetAsync(P.kctrl, 0, h->ndom * sizeof(KrylovCtrl), h->stream));
+    CK(cudaMemsetAsync(P.octrl, 0, h->ndom * sizeof(OverlandCtrl), h->stream));
+    CK(cudaMemsetAsync(P.diag, 0, h->ndom * sizeof(DevDiag), h->stream));
+    CK(cudaMemsetAsync(P.gctrl, 0, sizeof(GlobalCtrl), h->stream));
+    CK(cudaMemsetAsync(P.barrier, 0, sizeof(GridBarrier), h->stream));
+    CK(cudaMemsetAsync(P.arrive, 0, (size_t)h->ndom * 16, h->stream));
+    CK(launch_prepare(P, h->mixed, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->prepared = true;
+    return DHARA_OK;
+}
+
+int dhara_subsurface_step(dhara_handle *h) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    return enqueue_subsurface(h);
+}
+
+int dhara_overland_step(dhara_handle *h) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    return enqueue_overland(h);
+}
+
+int dhara_step(dhara_handle *h, int nsteps, int use_graph) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
+    if (nsteps < 0) return fail(DHARA_ERR_INVALID, "nsteps < 0");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    if (use_graph && !h->timing && !h->graph_failed && !h->graph_exec) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const long long lc = h->launch_count;
+        int rc = enqueue_subsurface(h);
+        if (!rc) rc = enqueue_overland(h);
+        cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        h->launch_count = lc;
+        if (rc == DHARA_OK && e == cudaSuccess) e = cudaGraphInstantiate(&h->graph_exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (rc != DHARA_OK || e != cudaSuccess) {
+            cudaGetLastError();
+            h->graph_exec = nullptr;
+            h->graph_failed = true;
+        }
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        if (use_graph && h->graph_exec && !h->timing) {
+            CK(cudaGraphLaunch(h->graph_exec, h->stream));
+            h->launch_count += 4 + 3 * (long long)h->maxiter_picard + 3;
+        } else {
+            int rc = enqueue_subsurface(h);
+            if (rc) return rc;
+            rc = enqueue_overland(h);
+            if (rc) return rc;
+        }
+    }
+    return DHARA_OK;
+}
+
+int dhara_synchronize(dhara_handle *h) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->stream));
+    return check_device_error(h);
+}
+
+int dhara_get_diagnostics(dhara_handle *h, int domain, dhara_diagnostics *out) {
+    if (!h || !out) return fail(DHARA_ERR_INVALID, "NULL argument");
+    if (domain < 0 || domain >= h->ndom) return fail(DHARA_ERR_INVALID, "domain out of range");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    DevDiag dg;
+    PicardCtrl pc;
+    CK(cudaMemcpyAsync(&dg, h->P.diag + domain, sizeof(dg), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&pc, h->P.pctrl + domain, sizeof(pc), cudaMemcpyDeviceToHost, h->stream));
+    int rc = check_device_error(h);
+    std::memset(out, 0, sizeof(*out));
+    out->steps = pc.step;
+    out->picard_iters_total = dg.picard_iters_total;
+    out->krylov_iters_total = dg.krylov_iters_total;
+    out->refine_iters_total = dg.refine_iters_total;
+    out->overland_iters_total = dg.overland_iters_total;
+    out->picard_iters_last = dg.picard_iters_last;
+    out->krylov_iters_last = dg.krylov_iters_last;
+    out->picard_nonconverged = dg.picard_nonconverged;
+    out->krylov_nonconverged = dg.krylov_nonconverged;
+    out->overland_nonconverged = dg.overland_nonconverged;
+    out->nonfinite = dg.nonfinite;
+    out->mb_subsurface_last = dg.mb_last;
+    out->mb_subsurface_cum = dg.mb_cum;
+    out->storage_change_cum = dg.storage_cum;
+    out->top_inflow_cum = dg.top_cum;
+    out->bottom_outflow_cum = dg.bottom_cum;
+    out->rain_cum = dg.rain_cum;
+    out->overland_boundary_out_cum = dg.olf_out_cum;
+    out->overland_clip_cum = dg.olf_clip_cum;
+    out->ponded_volume = dg.ponded;
+    out->picard_err_last = pc.err;
+    out->krylov_relres_last = dg.krylov_relres_last;
+    return rc;
+}
+
+int dhara_get_stream(dhara_handle *h, void **stream) {
+    if (!h || !stream) return fail(DHARA_ERR_INVALID, "NULL argument");
+    *stream = (void *)h->stream;
+    return DHARA_OK;
+}
+
+int dhara_set_kernel_timing(dhara_handle *h, int enable) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->stream));
+    collect_timing(h);
+    h->timing = enable != 0;
+    return DHARA_OK;
+}
+
+int dhara_get_kernel_timing(dhara_handle *h, int kernel, int64_t *launches, double *total_ms) {
+    if (!h || kernel < 0 || kernel >= KT_N) return fail(DHARA_ERR_INVALID, "bad kernel id");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->stream));
+    collect_timing(h);
+    if (launches) *launches = h->launches[kernel];
+    if (total_ms) *total_ms = h->total_ms[kernel];
+    return DHARA_OK;
+}
+
+int dhara_reset_kernel_timing(dhara_handle *h) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->stream));
+    collect_timing(h);
+    for (int k = 0; k < KT_N; ++k) {
+        h->total_ms[k] = 0;
+        h->launches[k] = 0;
+    }
+    h->launch_count = 0;
+    return DHARA_OK;
+}
+
+int dhara_get_launch_count(dhara_handle *h, int64_t *count) {
+    if (!h || !count) return fail(DHARA_ERR_INVALID, "NULL argument");
+    *count = h->launch_count;
+    return DHARA_OK;
+}
+
+int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    const double sT = h->mixed ? 4.0 : 8.0;
+    double total = 0.0;
+    int64_t iters = 0;
+    for (int d = 0; d < h->ndom; ++d) {
+        dhara_diagnostics dg;
+        int rc = dhara_get_diagnostics(h, d, &dg);
+        if (rc) return rc;
+        const DomainDesc &D = h->hdom[d];
+        const double N = (double)D.nx * D.ny * D.nz;
+        const double solves = (double)dg.picard_iters_total;
+        const double cycles = (double)dg.refine_iters_total;
+        const double upd = cycles > solves ? cycles - solves : 0.0;
+        // inner iteration: phase A 5 T-words, phase B 8 T-words; outer residual
+        // R: x, b, K64, D64 (f64) + r, z (T); update U: x read+write (f64) + d (T).
+        total += N * (13.0 * sT * (double)dg.krylov_iters_total + (32.0 + 2.0 * sT) * cycles +
+                      (16.0 + sT) * upd);
+        iters += dg.krylov_iters_total;
+    }
+    if (bytes) *bytes = total;
+    if (iterations) *iterations = iters;
+    return DHARA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,153 @@
+// internal.h -- shared host/device definitions of the B200 flow solver.
+//
+// Data model: all domains of a handle are concatenated in struct-of-arrays
+// device buffers in the reference layout (k-major, k = 0 top).  Work is
+// organised in COLUMN TILES of TILE_X x TILE_Y columns; a CUDA block owns one
+// tile at a time and each thread marches down one (i, j) column, so the
+// z-neighbours of the 7-point stencil stay in registers and the x/y
+// neighbours are coalesced loads along the same k-plane.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/dhara_gpu.h"
+
+#define TILE_X 32
+#define TILE_Y 4
+#define TILE_THREADS (TILE_X * TILE_Y)
+#define NZ_MAX 64
+
+// Per-domain constants (device copy in DevPtrs::dom).
+struct DomainDesc {
+    int nx, ny, nz, has_alpha;
+    int has_n, picard_rule, theta_update, picard_maxiter;
+    int krylov_maxiter, inner_maxiter, overland_maxiter, sched_len;
+    int tile_begin, tile_end, closure_fp32, pad1;
+    long long off3, off2, offWE, offSN, sched_off;
+    double dx, dy, dz, dt;
+    double alpha, n, theta_s, theta_r, porosity, Ss, am;
+    double delta, hmin, K0, sec;
+    double picard_tol, krylov_tol, inner_tol, overland_tol;
+};
+
+struct TileDesc {
+    int dom, x0, y0, pad;
+};
+
+// Per-domain solver control, written by exactly one block at a time (the last
+// block to finish a reduction for that domain) and read by all blocks after a
+// grid barrier.
+struct KrylovCtrl {
+    double bb;          // ||b||^2 of the 3D system
+    double rr64;        // ||b - A x||^2 at the last outer check
+    double rr;          // inner residual^2
+    double rz, rz_old;  // preconditioned inner products
+    double pAp, alpha, beta;
+    double inner_target2;
+    int active;         // outer solve still running
+    int inner_active;   // inner PCG running
+    int inner_iter;     // inner iterations in the current cycle
+    int total_iter;     // inner iterations this solve
+    int cycles;         // outer residual recomputes this solve
+    int parity;         // which p buffer holds the current direction
+    int first_inner;
+    int pad;
+};
+
+struct PicardCtrl {
+    int iter;           // Picard iterations done this step
+    int done;           // converged or capped
+    int converged;
+    int step;           // steps done (indexes the rain schedule)
+    double err;
+};
+
+struct OverlandCtrl {
+    double bb, rr, rz, rz_old, pAp, alpha, beta;
+    int active, iter, parity, pad;
+};
+
+// Diagnostics accumulated on the device (copied into dhara_diagnostics).
+struct DevDiag {
+    long long picard_iters_total, krylov_iters_total, refine_iters_total, overland_iters_total;
+    int picard_iters_last, krylov_iters_last, picard_nonconverged, krylov_nonconverged;
+    int overland_nonconverged, nonfinite, pad0, pad1;
+    double mb_last, mb_cum, storage_cum, top_cum, bottom_cum, rain_cum;
+    double olf_out_cum, olf_clip_cum, ponded, picard_err_last, krylov_relres_last;
+};
+
+struct GridBarrier {
+    unsigned int count;
+    unsigned int gen;
+    int error;
+    int pad;
+};
+
+// Global counters for the persistent kernels.
+struct GlobalCtrl {
+    int n_active;        // domains with an active outer solve
+    int n_inner_active;  // domains with an active inner solve
+    int n_olf_active;
+    int pad;
+};
+
+// Number of double partial sums per tile kept for reductions.
+#define NPART 12
+
+// Device pointers of a handle.  T-typed buffers are float in mixed mode and
+// double in FP64 mode; they are stored as void* and cast in the kernels.
+struct DevPtrs {
+    const DomainDesc *dom;
+    const TileDesc *tiles;
+    int ntiles, ndom;
+    // 3D double state
+    double *psin, *thetan, *psim, *x, *b, *ksat, *alpha, *nvg;
+    // FP64 coefficients of the outer residual (alias K, D in FP64 mode)
+    double *K64, *D64;
+    // 3D inner-precision buffers
+    void *K, *D, *r, *p0, *p1, *z, *d;
+    // 2D double
+    double *ztopo, *mann, *h, *H, *ph, *ppt, *esoil, *tr, *hpoten, *qtop, *ktop, *bcqb;
+    double *olf_k;       // 4*C: kw, ke, ks, kn per column (row-based)
+    double *olf_b, *olf_r, *olf_p0, *olf_p1, *olf_z;
+    // faces
+    double *bcqw, *bcqe, *bcqs, *bcqn;
+    int *procmap;
+    double *rda;         // [ndom][nproc_max*nz_max]
+    int nproc_max, rda_stride;
+    double *rain_sched;
+    // control
+    KrylovCtrl *kctrl;
+    PicardCtrl *pctrl;
+    OverlandCtrl *octrl;
+    DevDiag *diag;
+    GlobalCtrl *gctrl;
+    GridBarrier *barrier;
+    double *partials;    // [ntiles][NPART]
+    unsigned int *arrive;// [ndom][4]
+    double *step_acc;    // [ndom][16] per-step sums
+};
+
+// Host-side launchers (subsurface.cu / overland.cu).
+struct LaunchCfg {
+    int coop_blocks_3d;   // resident blocks for the persistent 3D solve
+    int coop_blocks_2d;
+    int smem_3d;          // dynamic shared memory bytes of the 3D solve
+    int nz_max;
+    int mixed;
+};
+
+cudaError_t launch_psi_from_theta(const DevPtrs &P, cudaStream_t s);
+cudaError_t launch_prepare(const DevPtrs &P, int mixed, cudaStream_t s);
+cudaError_t launch_prologue(const DevPtrs &P, cudaStream_t s);
+cudaError_t launch_assemble(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
+cudaError_t launch_krylov(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
+cudaError_t launch_picard_check(const DevPtrs &P, cudaStream_t s);
+cudaError_t launch_epilogue(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
+cudaError_t launch_eval_fields(const DevPtrs &P, int which, double *out, cudaStream_t s);
+cudaError_t launch_overland_setup(const DevPtrs &P, long long ctot, cudaStream_t s);
+cudaError_t launch_overland_solve(const DevPtrs &P, const LaunchCfg &L, long long ctot, cudaStream_t s);
+cudaError_t launch_overland_finish(const DevPtrs &P, long long ctot, cudaStream_t s);
+cudaError_t configure_3d(LaunchCfg &L, int device, int ntiles);
+cudaError_t configure_2d(LaunchCfg &L, int device);

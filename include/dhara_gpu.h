@@ -1,0 +1,244 @@
+/*
+ * dhara_gpu.h -- C ABI of the B200 integrated surface-subsurface flow solver.
+ *
+ * The library advances one or more independent domains of Dhara's coupled
+ * model: the 3D mixed-form Richards equation (modified Picard, van
+ * Genuchten-Mualem closure, implicit 7-point finite volumes) followed by the
+ * 2D diffusive-wave overland model (Manning conductances, implicit 5-point
+ * system with a fixed-elevation boundary ring), coupled through ponding and
+ * infiltration at the top boundary, exactly as one call of the reference's
+ *
+ *     SubsurfaceFlowModel(...)   src/subsurface.cu:686-847
+ *     OverlandFlowModel(...)     src/overland.cu:387-419
+ *
+ * does per time step inside RunCoupledFlowModel (src/device.cu:374-475).
+ *
+ * Array layouts are the reference's (include/class.h:99-217,
+ * src/numerical.cc:38-192):
+ *   3D cell   (i,j,k) -> k*nx*ny + j*nx + i, k = 0 is the TOP soil layer
+ *   2D column (i,j)   -> j*nx + i
+ *   W/E faces [nz*ny] at k*ny + j, S/N faces [nz*nx] at k*nx + i,
+ *   top/bottom faces [ny*nx] at j*nx + i            (src/subsurface.cu:139-142)
+ * Units are SI: metres, seconds, alpha in 1/m (the reference works in cm
+ * internally and converts, src/global.cu:79-97).
+ *
+ * Every entry point returns a dhara_status; nothing calls exit() or abort().
+ * A handle is used by one host thread at a time; all device work of a handle
+ * runs on the handle's own CUDA stream.
+ */
+#ifndef DHARA_GPU_H
+#define DHARA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DHARA_ABI_VERSION 1
+
+typedef enum {
+    DHARA_OK = 0,
+    DHARA_ERR_INVALID = 1,      /* bad argument, size or field */
+    DHARA_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    DHARA_ERR_NOMEM = 3,        /* device or host allocation failed */
+    DHARA_ERR_UNSUPPORTED = 4,  /* valid input this build does not handle */
+    DHARA_ERR_NONFINITE = 5,    /* NaN/Inf detected in the state */
+    DHARA_ERR_TIMEOUT = 6,      /* a bounded device-side wait ran out */
+    DHARA_ERR_STATE = 7         /* call out of order (e.g. step before upload) */
+} dhara_status;
+
+typedef enum { DHARA_FP64 = 0, DHARA_MIXED = 1 } dhara_precision;
+
+/* Picard stopping rule.  The reference's rule is relative
+ * max|(psi^{m+1}-psi^m)/psi^{m+1}| (PICARD_METHOD=0) or the same on theta
+ * (PICARD_METHOD=1), src/subsurface.cu:432-446,762-789. */
+typedef enum {
+    DHARA_PICARD_PSI_RELATIVE = 0,
+    DHARA_PICARD_THETA_RELATIVE = 1,
+    DHARA_PICARD_PSI_ABSOLUTE = 2
+} dhara_picard_rule;
+
+/* What becomes theta^n for the next step.  The reference copies thetanp1m,
+ * i.e. theta evaluated at the input of the last Picard iteration
+ * (src/subsurface.cu:839-840). */
+typedef enum {
+    DHARA_THETA_REFERENCE = 0,   /* theta(psi^m), as the reference */
+    DHARA_THETA_FINAL = 1,       /* theta(psi^{m+1}) */
+    DHARA_THETA_CONSERVATIVE = 2 /* theta^m + C^m (psi^{m+1} - psi^m): closes the discrete balance */
+} dhara_theta_update;
+
+/* Per-domain parameters.  Field names follow the reference's config keys
+ * (src/io.cc:236-274) and __constant__ set (include/devconst.h:6-31). */
+typedef struct {
+    int32_t struct_size;        /* = sizeof(dhara_params) */
+    int32_t nx, ny, nz;
+    double dx, dy, dz, dt;      /* m, m, m, s */
+    /* van Genuchten-Mualem, scalars (per-cell alpha/n may be uploaded) */
+    double alpha;               /* 1/m */
+    double n;                   /* pore-size distribution (PORE_SIZE_DISTRIBUTION) */
+    double theta_s, theta_r, porosity, Ss;
+    double airdry, psimin;      /* carried for completeness (unused by the path) */
+    double am;                  /* Picard relaxation psi^m <- am psi^m + (1-am) psi^{m+1}, 0 <= am < 1 */
+    /* overland (DELTA, WATERDEPTH_MINIMUM, WATERDEPTH_CRITICAL, KZERO) */
+    double delta, hmin, hcri, K0;
+    /* converts E_soil / TR rates into metres per step (sec_p_mm2dt_p_m) */
+    double sec_p_mm2dt_p_m;
+    /* Picard */
+    int32_t picard_maxiter;
+    int32_t picard_rule;        /* dhara_picard_rule */
+    double picard_tol;
+    /* 3D linear solve: stop when ||b - A x||_2 <= tol * ||b||_2 or maxiter */
+    int32_t krylov_maxiter;
+    int32_t theta_update;       /* dhara_theta_update */
+    double krylov_tol;
+    /* 2D overland linear solve */
+    int32_t overland_maxiter;
+    int32_t precision;          /* dhara_precision */
+    double overland_tol;
+    /* mixed precision: inner FP32 solve reduces the FP64 residual by this factor */
+    double inner_tol;
+    int32_t inner_maxiter;
+    /* mixed precision: 0 evaluates the van Genuchten closure in FP64 and the
+     * FP64 refinement residual uses FP64 coefficients (the converged head is
+     * the FP64 system's); 1 evaluates the closure in FP32 (faster; the
+     * refinement then converges to the FP32-coefficient system). */
+    int32_t closure_fp32;
+    int32_t reserved_i[6];
+    double reserved_d[8];
+} dhara_params;
+
+/* Fills p with the reference's device defaults (include/devconst.h) converted
+ * to SI with the given grid; dt in seconds. */
+void dhara_default_params(dhara_params *p, int nx, int ny, int nz,
+                          double dx, double dy, double dz, double dt);
+
+/* Data fields for upload/download.  Sizes: N = nx*ny*nz cells, C = nx*ny
+ * columns, FWE = nz*ny, FSN = nz*nx. */
+typedef enum {
+    /* 3D, double, N */
+    DHARA_F_PSI = 0,        /* psin: pressure head of the current state, m */
+    DHARA_F_THETA = 1,      /* thetan: moisture of the current state */
+    DHARA_F_KSAT = 2,       /* ksat, m/s */
+    DHARA_F_ALPHA = 3,      /* optional per-cell alpha, 1/m */
+    DHARA_F_NVG = 4,        /* optional per-cell n */
+    DHARA_F_K = 5,          /* knp1m: K at the last evaluation (download) */
+    DHARA_F_C = 6,          /* cnp1m (download) */
+    DHARA_F_THETA_NEW = 7,  /* thetanp1mp1: theta(psi^{m+1}) of the last step (download) */
+    /* 2D, double, C */
+    DHARA_F_ZTOPO = 16,
+    DHARA_F_MANN = 17,
+    DHARA_F_WATERDEPTH = 18,/* overland h */
+    DHARA_F_WATERELEV = 19, /* overland H = h + z */
+    DHARA_F_PONDING = 20,   /* ph */
+    DHARA_F_PPT = 21,       /* ppt_ground, mm per step */
+    DHARA_F_ESOIL = 22,     /* E_soil */
+    DHARA_F_TR = 23,        /* TR */
+    DHARA_F_HPOTEN = 24,    /* (download) */
+    DHARA_F_QTOP = 25,      /* bcqt: top flux of the last step (download) */
+    /* boundary values, double */
+    DHARA_F_BCQW = 32, DHARA_F_BCQE = 33,   /* FWE */
+    DHARA_F_BCQS = 34, DHARA_F_BCQN = 35,   /* FSN */
+    DHARA_F_BCQB = 36,                       /* C (overwritten by free drainage) */
+    DHARA_F_BCPSIW = 40, DHARA_F_BCPSIE = 41, DHARA_F_BCPSIS = 42, DHARA_F_BCPSIN = 43,
+    DHARA_F_BCPSIB = 44,
+    /* int32 fields */
+    DHARA_FI_BCW = 64, DHARA_FI_BCE = 65,   /* FWE */
+    DHARA_FI_BCS = 66, DHARA_FI_BCN = 67,   /* FSN */
+    DHARA_FI_BCB = 68, DHARA_FI_BCT = 69,   /* C */
+    DHARA_FI_PROCMAP = 70,                   /* C */
+    /* root density table, double, nproc*nz (set with dhara_set_roots) */
+    DHARA_F_ROOT = 80
+} dhara_field;
+
+typedef struct dhara_handle dhara_handle;
+
+typedef struct {
+    int64_t steps;                  /* time steps completed */
+    int64_t picard_iters_total;     /* Picard iterations over all steps */
+    int64_t krylov_iters_total;     /* inner (FP32 in mixed mode) Krylov iterations */
+    int64_t refine_iters_total;     /* FP64 residual recomputes (mixed mode) */
+    int64_t overland_iters_total;
+    int32_t picard_iters_last;
+    int32_t krylov_iters_last;      /* over all Picard iterations of the last step */
+    int32_t picard_nonconverged;    /* steps that hit picard_maxiter */
+    int32_t krylov_nonconverged;    /* linear solves that hit their iteration cap */
+    int32_t overland_nonconverged;
+    int32_t nonfinite;              /* 1 if NaN/Inf was seen */
+    double mb_subsurface_last;      /* reference water balance of the last step, m (src/subsurface.cu:809-826) */
+    double mb_subsurface_cum;       /* sum over steps of the above */
+    double storage_change_cum;      /* sum dz*(theta^{n+1}-theta^n) + specific storage, m per column area */
+    double top_inflow_cum;          /* sum dt*sum(q_top), m (column-summed) */
+    double bottom_outflow_cum;      /* sum dt*sum(q_bottom), m */
+    double rain_cum;                /* sum over columns of rain per step, m */
+    double overland_boundary_out_cum;   /* water leaving through the fixed ring, m */
+    double overland_clip_cum;       /* water created by h = max(H-z,0), m */
+    double ponded_volume;           /* sum h over columns after the last step, m */
+    double picard_err_last;         /* last Picard difference measure */
+    double krylov_relres_last;      /* last ||r||/||b|| of the 3D solve */
+    double reserved[6];
+} dhara_diagnostics;
+
+/* ---- lifetime ---------------------------------------------------------- */
+
+/* Creates a handle for ndomains independent domains, params[d] each.  All
+ * domains must share one precision and the same Picard/Krylov caps.  The
+ * handle owns all device memory.  device < 0 uses the current device. */
+int dhara_create(const dhara_params *params, int ndomains, int device, dhara_handle **out);
+int dhara_destroy(dhara_handle *h);
+
+/* Message of the last failing call on this thread (never NULL). */
+const char *dhara_last_error(void);
+int dhara_abi_version(void);
+
+/* ---- data in / out (host buffers; copies complete before return) ------ */
+
+int dhara_upload(dhara_handle *h, int domain, int field, const double *src, int64_t count);
+int dhara_upload_int(dhara_handle *h, int domain, int field, const int32_t *src, int64_t count);
+int dhara_download(dhara_handle *h, int domain, int field, double *dst, int64_t count);
+/* Root density table rda[proc*nz + k] (src/subsurface.cu:115). */
+int dhara_set_roots(dhara_handle *h, int domain, const double *rda, int nproc);
+/* Optional per-step rain for graph-replayed runs: mm per step, uniform over
+ * the domain, used instead of the PPT field for steps [0, nsteps). */
+int dhara_set_rain_schedule(dhara_handle *h, int domain, const double *mm_per_step, int nsteps);
+
+/* ---- the hot path -------------------------------------------------------- */
+
+/* CopyDataToDevice's theta->psi conversion, vanGenuchtenInverse
+ * (src/device.cu:327, src/global.cu:32-52): psi := psi(theta) for every domain. */
+int dhara_psi_from_theta(dhara_handle *h);
+
+/* PreRunningFlowModel (src/global.cu:270-296): evaluates theta, K, C at psi
+ * and resets per-step state.  Must follow the uploads, precede stepping. */
+int dhara_prepare(dhara_handle *h);
+
+/* One reference SubsurfaceFlowModel call for every domain (no host sync). */
+int dhara_subsurface_step(dhara_handle *h);
+/* One reference OverlandFlowModel call for every domain (no host sync). */
+int dhara_overland_step(dhara_handle *h);
+/* nsteps x (subsurface step + overland step).  use_graph != 0 captures one
+ * step into a CUDA graph on first use and replays it. */
+int dhara_step(dhara_handle *h, int nsteps, int use_graph);
+
+int dhara_synchronize(dhara_handle *h);
+int dhara_get_diagnostics(dhara_handle *h, int domain, dhara_diagnostics *out);
+/* The cudaStream_t of the handle, for callers that time or order work. */
+int dhara_get_stream(dhara_handle *h, void **stream);
+
+/* Per-kernel CUDA-event timing (off by default).  kernel: 0 = 3D Krylov solve,
+ * 1 = Picard assembly, 2 = Picard check, 3 = step epilogue, 4 = overland solve,
+ * 5 = overland set-up/finish, 6 = step prologue. */
+int dhara_set_kernel_timing(dhara_handle *h, int enable);
+int dhara_get_kernel_timing(dhara_handle *h, int kernel, int64_t *launches, double *total_ms);
+int dhara_reset_kernel_timing(dhara_handle *h);
+/* Kernel launches this handle has issued (graph replays count their nodes). */
+int dhara_get_launch_count(dhara_handle *h, int64_t *count);
+/* Algorithmic HBM bytes moved by the 3D Krylov kernel so far (the count the
+ * roofline figure divides by time), and the inner iterations they cover. */
+int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DHARA_GPU_H */
