@@ -1,0 +1,402 @@
+"""Benchmark: coupled surface-subsurface flow steps per second on B200.
+
+Workload (default): one 512x512x40 hillslope domain (10,485,760 cells),
+mixed precision (FP32 inner Krylov iterations, FP64 refinement, FP64 closure
+and mass accumulator), rain 20 mm/h for 2 h then 2 h recession, dt = 60 s;
+the timed region is K time steps from the initial state (K = 240 is the whole
+storm).  A "step" is one time step of the coupled model for the domain: the
+Picard loop (assembly, persistent Krylov solve, convergence check), the step
+epilogue, and the overland solve.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (launched by torchrun) every rank runs an independent replica of
+the domain on its own GPU ("replicas only": the single-domain solve does not
+shard); value is the aggregate over ranks, timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s mixed vs FP64 on 1 B200 at <=1e-8 mass error; adjoint/fwd time"
+UNIT = "cell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=240)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--nz", type=int, default=40)
+    ap.add_argument("--fp64-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_cell_iter():
+    """DRAM bytes per cell per inner Krylov iteration measured by ncu on the
+    same kernel (profiles/krylov_traffic.json, written from an ncu capture)."""
+    p = os.path.join(ROOT, "profiles", "krylov_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ ours
+def run_ours(args, world, rank, local):
+    import torch
+    import dhara_b200 as db
+    from dhara_b200 import inputs
+
+    torch.cuda.set_device(local)
+    dom = inputs.mixed_512x512x40(nx=args.nx, ny=args.nx, nz=args.nz, nsteps=max(args.steps, 1))
+    N = dom.ncells
+    p = dom.params
+
+    def fresh(precision=db.MIXED):
+        q = type(p).from_buffer_copy(p)
+        q.precision = precision
+        s = db.Solver(q, device=local)
+        s.load(dom)
+        s.prepare()
+        return s
+
+    def timed(s, nsteps, graph=False, kernel_timing=False):
+        stream = torch.cuda.ExternalStream(s.stream, device=local)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        s.synchronize()
+        if kernel_timing:
+            s.set_kernel_timing(True)
+            s.reset_kernel_timing()
+        lc0 = s.launch_count()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.step(nsteps, graph=graph)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = e0.elapsed_time(e1)
+        return ms, s.launch_count() - lc0
+
+    # warm-up on a separate handle (same shapes), then a fresh state for timing
+    s = fresh()
+    s.step(args.warmup)
+    s.synchronize()
+    s.close()
+
+    s = fresh()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, launches = timed(s, args.steps, kernel_timing=True)
+    clk = clocks.stop()
+    dg = s.diagnostics()
+    kn, kms = s.kernel_timing("krylov")
+    kbytes, kiters = s.krylov_traffic()
+    timing = {k: s.kernel_timing(k) for k in db.KERNELS}
+    s.close()
+    ms_max = max_over_ranks(ms, world)
+    value = world * N * args.steps / (ms_max / 1e3)
+
+    # FP64 solver on the same workload (bounded number of steps)
+    fp64_value = None
+    if args.fp64_steps > 0:
+        s64 = fresh(db.FP64)
+        s64.step(1)
+        s64.synchronize()
+        s64.close()
+        s64 = fresh(db.FP64)
+        ms64, _ = timed(s64, min(args.fp64_steps, args.steps))
+        s64.close()
+        ms64 = max_over_ranks(ms64, world)
+        fp64_value = world * N * min(args.fp64_steps, args.steps) / (ms64 / 1e3)
+    # the same mixed steps for comparison over the same horizon
+    s2 = fresh()
+    ms_h, _ = timed(s2, min(args.fp64_steps, args.steps))
+    s2.close()
+    ms_h = max_over_ranks(ms_h, world)
+    mixed_same_horizon = world * N * min(args.fp64_steps, args.steps) / (ms_h / 1e3)
+
+    # end to end through the public API: per step upload the step's rain field
+    # from pinned host memory, advance, read back the ponded depth and the
+    # diagnostics record.
+    C = p.nx * p.ny
+    e2e = None
+    if args.e2e_steps > 0:
+        s3 = fresh()
+        q = type(p).from_buffer_copy(p)
+        rain_pinned = torch.empty(C, dtype=torch.float64, pin_memory=True).numpy()
+        pond_pinned = torch.empty(C, dtype=torch.float64, pin_memory=True).numpy()
+        ne = min(args.e2e_steps, args.steps)
+        # the rain field replaces the schedule: clear the schedule for this handle
+        s3.set_rain_schedule(np.zeros(0))
+        stream = torch.cuda.ExternalStream(s3.stream, device=local)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        t0 = time.perf_counter()
+        for t in range(ne):
+            rain_pinned[:] = dom.rain_mm[t]
+            s3.upload("ppt", rain_pinned)
+            s3.step(1)
+            import ctypes as ct
+            rc = db.lib().dhara_download(s3.h, 0, db._abi.F["ponding"],
+                                         pond_pinned.ctypes.data_as(ct.POINTER(ct.c_double)), C)
+            if rc != 0:
+                raise RuntimeError(db.lib().dhara_last_error().decode())
+            s3.diagnostics()
+        e1.record(stream)
+        e1.synchronize()
+        wall = time.perf_counter() - t0
+        barrier(world)
+        ms_e = max_over_ranks(max(e0.elapsed_time(e1), wall * 1e3), world)
+        s3.close()
+        e2e = {"value": world * N * ne / (ms_e / 1e3), "unit": UNIT, "steps": ne,
+               "h2d_bytes_per_step": C * 8, "d2h_bytes_per_step": C * 8 + 312,
+               "path": "dhara_upload(ppt) + dhara_step(1) + dhara_download(ponding) + "
+                       "dhara_get_diagnostics, pinned host buffers"}
+
+    # roofline of the dominant kernel (the persistent Krylov solve)
+    peak, peak_kind = measured_peak()
+    # algorithmic bytes of the timed region only (the counter is cumulative
+    # per handle and this handle was created fresh for the timed region)
+    achieved = (kbytes / (kms / 1e3)) / 1e9 if kms > 0 else None
+    ncu = ncu_traffic_per_cell_iter()
+    traffic = None
+    if ncu and kn > 0 and kiters > 0:
+        traffic = ncu["dram_bytes_per_cell_iter"] * N * (kiters / kn)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_krylov<float>",
+                "algorithmic_bytes_per_launch": kbytes / kn if kn else None,
+                "avg_launch_ms": kms / kn if kn else None,
+                "launches": kn, "share_of_step": kms / ms if ms else None}
+
+    mass_err = dg["storage_change_cum"] - (dg["top_inflow_cum"] - dg["bottom_outflow_cum"])
+    inflow = dg["top_inflow_cum"]
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner Krylov + f64 refinement/closure",
+        "data": "synthetic (seeded GRF topography, lognormal Ks; no public dataset)",
+        "config": {"workload": f"mixed_{p.nx}x{p.ny}x{p.nz}", "cells": N, "dt_s": p.dt,
+                   "storm": "20 mm/h for 2 h then recession", "precision": "mixed",
+                   "picard": "absolute 1e-6 m, max 10, am 0.25", "krylov_tol": p.krylov_tol,
+                   "l2": "inputs larger than L2 (~0.8 GB working set per step)",
+                   "parallelism": f"replicas x{world}"},
+        "fp64_value": fp64_value, "mixed_same_horizon": mixed_same_horizon,
+        "speedup_mixed_vs_fp64": (mixed_same_horizon / fp64_value) if fp64_value else None,
+        "mass_error_over_inflow": mass_err / inflow if inflow else None,
+        "picard_iters": dg["picard_iters_total"], "krylov_inner_iters": dg["krylov_iters_total"],
+        "refine_cycles": dg["refine_iters_total"], "overland_iters": dg["overland_iters_total"],
+        "adjoint_over_forward": None,
+        "kernel_ms": {k: v[1] for k, v in timing.items()},
+        "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args)
+    return out
+
+
+# ------------------------------------------------------------ CPU oracle
+def cpu_sample_domain(args, n=64):
+    """The bounded CPU sample: the same physics, solver settings and forcing on
+    an n x n patch (same nz) of the benchmark domain's configuration."""
+    from dhara_b200 import inputs
+    return inputs.mixed_512x512x40(nx=n, ny=n, nz=args.nz, precision=0, nsteps=max(args.steps, 8))
+
+
+def cpu_baseline(args, sample_steps=8, threads=None):
+    import oracle
+    threads = threads or os.cpu_count() or 1
+    oracle.set_threads(threads)
+    d = cpu_sample_domain(args)
+    o = oracle.Oracle(d.params, oracle.SOLVER_BICGSTAB, oracle.SOLVER_CG)
+    o.load(d)
+    o.prepare()
+    t0 = time.perf_counter()
+    for t in range(sample_steps):
+        o.step(d.rain_mm[t])
+    dt = time.perf_counter() - t0
+    o.close()
+    n = d.ncells * sample_steps
+    return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"FP64 oracle (reference algorithm: unpreconditioned BiCGSTAB, CUSP rules) "
+                      f"on a {d.params.nx}x{d.params.ny}x{d.params.nz} patch of the workload, "
+                      f"{sample_steps} step(s), {dt:.2f} s, {threads} OpenMP threads"}
+
+
+def run_reference(args, world, rank):
+    """The reference's algorithm on the host cores (the reference's own CPU
+    path does not exist and its CUSP dependency does not build here, so the
+    FP64 oracle port stands in); each step is one time step of a bounded
+    patch of the workload."""
+    if rank != 0:
+        return None
+    import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    d = cpu_sample_domain(args, n=32)
+    o = oracle.Oracle(d.params, oracle.SOLVER_BICGSTAB, oracle.SOLVER_CG)
+    o.load(d)
+    o.prepare()
+    for t in range(args.warmup):
+        o.step(d.rain_mm[t % len(d.rain_mm)])
+    o.close()
+    o = oracle.Oracle(d.params, oracle.SOLVER_BICGSTAB, oracle.SOLVER_CG)
+    o.load(d)
+    o.prepare()
+    budget_s = 240.0
+    t0 = time.perf_counter()
+    done = 0
+    for t in range(args.steps):
+        o.step(d.rain_mm[t % len(d.rain_mm)])
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    v = d.ncells * done / dt
+    sample = (f"FP64 oracle port of the reference algorithm on a {d.params.nx}x{d.params.ny}x"
+              f"{d.params.nz} patch of the workload, {done} of {args.steps} steps timed "
+              f"({dt:.1f} s), {threads} OpenMP threads")
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": done,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(done, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"mixed_{args.nx}x{args.nx}x{args.nz} (CPU patch "
+                                   f"{d.params.nx}x{d.params.ny}x{d.params.nz})"},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            out = run_reference(args, world, rank)
+        else:
+            out = run_ours(args, world, rank, local)
+        if rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -10,6 +10,8 @@
 // device, so the sequence can be captured once into a CUDA graph and replayed.
 #include "internal.h"
 
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -221,6 +223,7 @@ struct FieldLoc {
     bool is_int;
     bool computed;  // download evaluates the closure
     int which;
+    bool is3d;      // pitched 3D array (rows of nx values at pitch nxp)
 };
 
 int locate(dhara_handle *h, int dom, int field, FieldLoc *out) {
@@ -229,7 +232,7 @@ int locate(dhara_handle *h, int dom, int field, FieldLoc *out) {
     const long long N = (long long)D.nx * D.ny * D.nz, C = (long long)D.nx * D.ny;
     const long long WE = (long long)D.nz * D.ny, SN = (long long)D.nz * D.nx;
     DevPtrs &P = h->P;
-    FieldLoc f{nullptr, 0, sizeof(double), false, false, 0};
+    FieldLoc f{nullptr, 0, sizeof(double), false, false, 0, false};
     switch (field) {
         case DHARA_F_PSI: f.ptr = P.psin + D.off3; f.count = N; break;
         case DHARA_F_THETA: f.ptr = P.thetan + D.off3; f.count = N; break;
@@ -267,6 +270,7 @@ int locate(dhara_handle *h, int dom, int field, FieldLoc *out) {
         case DHARA_FI_PROCMAP: f.ptr = P.procmap + D.off2; f.count = C; f.is_int = true; f.elt = 4; break;
         default: return fail(DHARA_ERR_INVALID, "unknown field id %d", field);
     }
+    f.is3d = field <= DHARA_F_THETA_NEW;
     *out = f;
     return DHARA_OK;
 }
@@ -275,6 +279,82 @@ int upload_dom_desc(dhara_handle *h) {
     CK(cudaMemcpyAsync(h->d_dom, h->hdom.data(), sizeof(DomainDesc) * h->ndom, cudaMemcpyHostToDevice,
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    return DHARA_OK;
+}
+
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// One 3D tiled map over a domain's part of a pitched array: dims (nx, ny, nz),
+// row pitch nxp; box (TILE_X + 2*xoff, TILE_Y + 2, chunk) for halo reads or
+// (TILE_X, TILE_Y, chunk) for own-column reads.  Out-of-range elements read as
+// zero.
+int encode_map(CUtensorMap *m, const void *array, size_t elt, const DomainDesc &D, bool halo, int chunk) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return fail(DHARA_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[3] = {(cuuint64_t)D.nx, (cuuint64_t)D.ny, (cuuint64_t)D.nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)D.nxp * elt, (cuuint64_t)D.nxp * D.ny * elt};
+    const int xoff = (int)(16 / elt);
+    const cuuint32_t box[3] = {(cuuint32_t)(halo ? TILE_X + 2 * xoff : TILE_X), (cuuint32_t)(halo ? TILE_Y + 2 : TILE_Y),
+                               (cuuint32_t)chunk};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    void *base = (void *)((const char *)array + (size_t)D.off3 * elt);
+    if (((uintptr_t)base & 15) != 0 || (strides[0] & 15) != 0)
+        return fail(DHARA_ERR_INVALID, "internal: unaligned 3D array for TMA");
+    CUresult r = enc(m, elt == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base,
+                     dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(DHARA_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return DHARA_OK;
+}
+
+int build_tensor_maps(dhara_handle *h) {
+    const DevPtrs &P = h->P;
+    const size_t sT = h->mixed ? 4 : 8;
+    const int chi = h->mixed ? CHUNK_F32 : CHUNK_F64;
+    std::vector<CUtensorMap> maps((size_t)h->ndom * NMAP);
+    for (int d = 0; d < h->ndom; ++d) {
+        const DomainDesc &D = h->hdom[d];
+        CUtensorMap *m = &maps[(size_t)d * NMAP];
+        int rc = 0;
+        rc |= encode_map(m + MAP_P0_H, P.p0, sT, D, true, chi);
+        rc |= encode_map(m + MAP_P1_H, P.p1, sT, D, true, chi);
+        rc |= encode_map(m + MAP_Z_H, P.z, sT, D, true, chi);
+        rc |= encode_map(m + MAP_K_H, P.K, sT, D, true, chi);
+        rc |= encode_map(m + MAP_D_O, P.D, sT, D, false, chi);
+        rc |= encode_map(m + MAP_DD_O, P.d, sT, D, false, chi);
+        rc |= encode_map(m + MAP_R_O, P.r, sT, D, false, chi);
+        rc |= encode_map(m + MAP_P0_O, P.p0, sT, D, false, chi);
+        rc |= encode_map(m + MAP_P1_O, P.p1, sT, D, false, chi);
+        rc |= encode_map(m + MAP_Q_O, P.q, sT, D, false, chi);
+        rc |= encode_map(m + MAP_INV_O, P.finv, sT, D, false, chi);
+        rc |= encode_map(m + MAP_E_O, P.fe, sT, D, false, chi);
+        rc |= encode_map(m + MAP_X64_H, P.x, 8, D, true, CH_R);
+        rc |= encode_map(m + MAP_K64_H, P.K64, 8, D, true, CH_R);
+        rc |= encode_map(m + MAP_D64_O, P.D64, 8, D, false, CH_R);
+        rc |= encode_map(m + MAP_B_O, P.b, 8, D, false, CH_R);
+        if (rc) return rc;
+    }
+    CUtensorMap *dm = nullptr;
+    if (dalloc(h, &dm, maps.size())) return DHARA_ERR_NOMEM;
+    CK(cudaMemcpyAsync(dm, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->P.tmaps = dm;
     return DHARA_OK;
 }
 
@@ -343,8 +423,10 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         D.picard_maxiter = p.picard_maxiter; D.krylov_maxiter = p.krylov_maxiter;
         D.overland_maxiter = p.overland_maxiter;
         D.inner_maxiter = h->mixed ? (p.inner_maxiter > 0 ? p.inner_maxiter : p.krylov_maxiter) : p.krylov_maxiter;
+        D.nxp = (p.nx + 3) & ~3;
+        h->Ntot = (h->Ntot + 31) & ~31LL;  // 128-byte aligned base for FP32 and FP64
         D.off3 = h->Ntot; D.off2 = h->Ctot; D.offWE = h->WEtot; D.offSN = h->SNtot;
-        h->Ntot += (long long)p.nx * p.ny * p.nz;
+        h->Ntot += (long long)D.nxp * p.ny * p.nz;
         h->Ctot += (long long)p.nx * p.ny;
         h->WEtot += (long long)p.nz * p.ny;
         h->SNtot += (long long)p.nz * p.nx;
@@ -376,7 +458,8 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     TileDesc *d_tiles = nullptr;
     rc |= dalloc(h, &d_tiles, h->htiles.size());
     for (double **q : {&P.psin, &P.thetan, &P.psim, &P.x, &P.b, &P.ksat}) rc |= dalloc(h, q, N);
-    for (void **q : {&P.K, &P.D, &P.r, &P.p0, &P.p1, &P.z, &P.d}) rc |= dalloc_void(h, q, N * sT);
+    for (void **q : {&P.K, &P.D, &P.r, &P.p0, &P.p1, &P.z, &P.d, &P.q, &P.finv, &P.fe, &P.fc})
+        rc |= dalloc_void(h, q, N * sT);
     if (h->mixed) {
         rc |= dalloc(h, &P.K64, N);
         rc |= dalloc(h, &P.D64, N);
@@ -410,6 +493,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     P.tiles = d_tiles;
     P.ntiles = (int)h->htiles.size();
     P.ndom = ndomains;
+    P.smem_nz = h->nz_max;
     P.alpha = P.nvg = nullptr;
     P.rain_sched = nullptr;
 
@@ -420,7 +504,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     auto zero = [&](void *p, size_t bytes) { return cudaMemsetAsync(p, 0, bytes, h->stream); };
     cudaError_t e = cudaSuccess;
     for (double *q : {P.psin, P.thetan, P.psim, P.x, P.b, P.ksat}) e = e ? e : zero(q, N * 8);
-    for (void *q : {P.K, P.D, P.r, P.p0, P.p1, P.z, P.d}) e = e ? e : zero(q, N * sT);
+    for (void *q : {P.K, P.D, P.r, P.p0, P.p1, P.z, P.d, P.q, P.finv, P.fe, P.fc}) e = e ? e : zero(q, N * sT);
     for (double *q : {P.K64, P.D64}) e = e ? e : zero(q, N * 8);
     for (double *q : {P.ztopo, P.mann, P.h, P.H, P.ph, P.ppt, P.esoil, P.tr, P.hpoten, P.qtop, P.ktop, P.bcqb,
                       P.olf_b, P.olf_r, P.olf_p0, P.olf_p1, P.olf_z})
@@ -446,6 +530,10 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
                         h->stream) != cudaSuccess)
         return bail(fail(DHARA_ERR_CUDA, "tile upload failed"));
     if (upload_dom_desc(h)) return bail(DHARA_ERR_CUDA);
+    {
+        const int rc2 = build_tensor_maps(h);
+        if (rc2) return bail(rc2);
+    }
 
     h->L.nz_max = h->nz_max;
     h->L.mixed = h->mixed;
@@ -487,7 +575,14 @@ int dhara_upload(dhara_handle *h, int domain, int field, const double *src, int6
         if (!std::isfinite(src[i]))
             return fail(DHARA_ERR_NONFINITE, "field %d value %lld is not finite", field, (long long)i);
     if (!f.ptr) return DHARA_OK;  // Dirichlet values: only meaningful with Dirichlet faces
-    CK(cudaMemcpyAsync(f.ptr, src, count * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (f.is3d) {
+        const DomainDesc &D = h->hdom[domain];
+        CK(cudaMemcpy2DAsync(f.ptr, (size_t)D.nxp * sizeof(double), src, (size_t)D.nx * sizeof(double),
+                             (size_t)D.nx * sizeof(double), (size_t)D.ny * D.nz, cudaMemcpyHostToDevice,
+                             h->stream));
+    } else {
+        CK(cudaMemcpyAsync(f.ptr, src, count * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    }
     CK(cudaStreamSynchronize(h->stream));
     if (field == DHARA_F_ALPHA || field == DHARA_F_NVG) {
         if (field == DHARA_F_ALPHA) h->hdom[domain].has_alpha = 1;
@@ -543,7 +638,13 @@ int dhara_download(dhara_handle *h, int domain, int field, double *dst, int64_t 
         f.ptr = h->scratch + D.off3;
     }
     if (!f.ptr) return fail(DHARA_ERR_INVALID, "field %d is not stored on the GPU path", field);
-    CK(cudaMemcpyAsync(dst, f.ptr, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (f.is3d) {
+        CK(cudaMemcpy2DAsync(dst, (size_t)D.nx * sizeof(double), f.ptr, (size_t)D.nxp * sizeof(double),
+                             (size_t)D.nx * sizeof(double), (size_t)D.ny * D.nz, cudaMemcpyDeviceToHost,
+                             h->stream));
+    } else {
+        CK(cudaMemcpyAsync(dst, f.ptr, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
     CK(cudaStreamSynchronize(h->stream));
     return DHARA_OK;
 }
@@ -778,9 +879,11 @@ int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations
         const double solves = (double)dg.picard_iters_total;
         const double cycles = (double)dg.refine_iters_total;
         const double upd = cycles > solves ? cycles - solves : 0.0;
-        // inner iteration: phase A 5 T-words, phase B 8 T-words; outer residual
-        // R: x, b, K64, D64 (f64) + r, z (T); update U: x read+write (f64) + d (T).
-        total += N * (13.0 * sT * (double)dg.krylov_iters_total + (32.0 + 2.0 * sT) * cycles +
+        // inner iteration: phase A reads z, p_old, K, D and writes p, q (6 T-words);
+        // phase B reads p, q, d, r, 1/den, a/den, c/den and writes d, r, z (10);
+        // outer residual R: x, b, K64, D64 (f64) + writes r, z and the three
+        // factors (5 T) + c/den read back (1 T); update U: x read+write (f64) + d (T).
+        total += N * (16.0 * sT * (double)dg.krylov_iters_total + (32.0 + 6.0 * sT) * cycles +
                       (16.0 + sT) * upd);
         iters += dg.krylov_iters_total;
     }

@@ -29,6 +29,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // another block reported an error; the caller must then return.
 __device__ __forceinline__ bool grid_sync(GridBarrier *gb) {
     __shared__ int s_ok;
+    // global writes of this phase are read by TMA (async proxy) in the next
+    asm volatile("fence.proxy.async.global;\n" ::: "memory");
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
@@ -126,7 +128,7 @@ __device__ __forceinline__ bool domain_reduce(const DevPtrs &P, int tile, int do
     }
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int i = 0; i < NV; ++i) __stcg(&P.partials[(size_t)tile * NPART + i], v[i]);
+        for (int i = 0; i < NV; ++i) __stcg(&P.partials[(size_t)i * P.ntiles + tile], v[i]);
         __threadfence();
         const DomainDesc &D = P.dom[dom];
         const unsigned int prev = atomicAdd(&P.arrive[dom * 4 + slot], 1u);
@@ -141,10 +143,13 @@ __device__ __forceinline__ bool domain_reduce(const DevPtrs &P, int tile, int do
     double acc[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = IS_MAX ? -INFINITY : 0.0;
+    // SoA partials: consecutive threads read consecutive tiles (coalesced) and
+    // the loop carries no dependence, so several loads are in flight.
+#pragma unroll 4
     for (int t = D.tile_begin + threadIdx.x; t < D.tile_end; t += blockDim.x) {
 #pragma unroll
         for (int i = 0; i < NV; ++i) {
-            const double w = __ldcg(&P.partials[(size_t)t * NPART + i]);
+            const double w = __ldcg(&P.partials[(size_t)i * P.ntiles + t]);
             acc[i] = IS_MAX ? fmax(acc[i], w) : acc[i] + w;
         }
     }
@@ -253,7 +258,7 @@ __device__ __forceinline__ double vg_theta(double psi, double alpha_m, double n,
 
 // Column geometry of a thread inside its tile.
 struct ColumnRef {
-    int dom, i, j, nx, ny, nz;
+    int dom, i, j, nx, ny, nz, nxp;
     long long g0, sxy;   // cell (i,j,0) index and plane stride
     long long c;         // column index in 2D arrays
     bool valid;
@@ -269,9 +274,10 @@ __device__ __forceinline__ ColumnRef column_of(const DevPtrs &P, int tile) {
     r.nx = D.nx;
     r.ny = D.ny;
     r.nz = D.nz;
+    r.nxp = D.nxp;
     r.valid = (r.i < D.nx) && (r.j < D.ny);
-    r.sxy = (long long)D.nx * D.ny;
-    r.g0 = D.off3 + (long long)r.j * D.nx + r.i;
+    r.sxy = (long long)D.nxp * D.ny;
+    r.g0 = D.off3 + (long long)r.j * D.nxp + r.i;
     r.c = D.off2 + (long long)r.j * D.nx + r.i;
     return r;
 }

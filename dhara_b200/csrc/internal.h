@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/dhara_gpu.h"
@@ -17,13 +18,31 @@
 #define TILE_Y 4
 #define TILE_THREADS (TILE_X * TILE_Y)
 #define NZ_MAX 64
+// planes per TMA-staged chunk: inner phases (by inner precision) and the FP64 residual
+#define CHUNK_F32 4
+#define CHUNK_F64 2
+#define CH_R 2
 
-// Per-domain constants (device copy in DevPtrs::dom).
+// Tensor maps of one domain (index = dom * NMAP + id): halo boxes
+// (TILE_X + 32 bytes) x (TILE_Y + 2) x chunk, own boxes TILE_X x TILE_Y x chunk.
+enum {
+    MAP_P0_H = 0, MAP_P1_H, MAP_Z_H, MAP_K_H,      // inner precision, halo boxes
+    MAP_D_O, MAP_DD_O, MAP_R_O,                    // inner precision, own boxes (D, d, r)
+    MAP_P0_O, MAP_P1_O, MAP_Q_O, MAP_INV_O, MAP_E_O,  // inner precision, own boxes
+    MAP_X64_H, MAP_K64_H, MAP_D64_O, MAP_B_O,      // FP64 outer residual
+    NMAP
+};
+
+// Per-domain constants (device copy in DevPtrs::dom).  3D arrays are stored
+// k-major like the reference, with the row pitch nxp = nx rounded up to a
+// multiple of 4 and every domain's base 128-byte aligned, so rows and planes
+// start on 16-byte boundaries (the TMA stride rule); columns i >= nx are
+// padding that no kernel reads as data.
 struct DomainDesc {
     int nx, ny, nz, has_alpha;
     int has_n, picard_rule, theta_update, picard_maxiter;
     int krylov_maxiter, inner_maxiter, overland_maxiter, sched_len;
-    int tile_begin, tile_end, closure_fp32, pad1;
+    int tile_begin, tile_end, closure_fp32, nxp;  // nxp: row pitch of 3D arrays (nx rounded up to 4)
     long long off3, off2, offWE, offSN, sched_off;
     double dx, dy, dz, dt;
     double alpha, n, theta_s, theta_r, porosity, Ss, am;
@@ -101,12 +120,17 @@ struct DevPtrs {
     const DomainDesc *dom;
     const TileDesc *tiles;
     int ntiles, ndom;
+    int smem_nz;         // column capacity of the Thomas buffers in shared memory
+    int pad_smem;
     // 3D double state
     double *psin, *thetan, *psim, *x, *b, *ksat, *alpha, *nvg;
     // FP64 coefficients of the outer residual (alias K, D in FP64 mode)
     double *K64, *D64;
     // 3D inner-precision buffers
     void *K, *D, *r, *p0, *p1, *z, *d;
+    // A p of the current direction, and the column preconditioner's stored
+    // Thomas factors (1/den, a/den, c/den), computed once per outer cycle
+    void *q, *finv, *fe, *fc;
     // 2D double
     double *ztopo, *mann, *h, *H, *ph, *ppt, *esoil, *tr, *hpoten, *qtop, *ktop, *bcqb;
     double *olf_k;       // 4*C: kw, ke, ks, kn per column (row-based)
@@ -124,9 +148,10 @@ struct DevPtrs {
     DevDiag *diag;
     GlobalCtrl *gctrl;
     GridBarrier *barrier;
-    double *partials;    // [ntiles][NPART]
+    double *partials;    // [NPART][ntiles] (structure of arrays)
     unsigned int *arrive;// [ndom][4]
     double *step_acc;    // [ndom][16] per-step sums
+    const CUtensorMap *tmaps;  // [ndom][NMAP] TMA descriptors of the 3D arrays
 };
 
 // Host-side launchers (subsurface.cu / overland.cu).

@@ -1,0 +1,121 @@
+// staging.cuh -- TMA staging of a column tile's z-planes into shared memory.
+//
+// A block owns a tile of TILE_X x TILE_Y columns and marches down k.  Each
+// input array of a sweep is copied chunk by chunk (CH planes at a time) into
+// shared memory by the Tensor Memory Accelerator: one thread arms the chunk's
+// mbarrier with the expected byte count and issues one
+// cp.async.bulk.tensor.3d per array; all threads wait on the mbarrier.  Two
+// buffers alternate, so chunk s+1 streams in while chunk s is consumed.
+//
+// Boxes (x, y, z), all starting at 16-byte aligned x (the TMA rule):
+//   halo arrays (read at x/y neighbours): x from x0 - XOFF, width
+//     BW = TILE_X + 2*XOFF with XOFF = 16 / sizeof(element), y from y0 - 1,
+//     height TILE_Y + 2;  shared layout [CH][TILE_Y+2][BW]
+//   own arrays (read at the thread's column): x0, y0, TILE_X x TILE_Y;
+//     shared layout [CH][TILE_Y*TILE_X]
+// Coordinates outside the domain (including the negative halo origin) are
+// zero-filled by the TMA unit.  Loads only, never multicast.
+#pragma once
+
+#include <cuda.h>
+
+#include "device_common.cuh"
+
+#define HY (TILE_Y + 2)
+#define OWN_PLANE TILE_THREADS
+
+template <typename V>
+struct Halo {
+    static constexpr int XOFF = 16 / (int)sizeof(V);
+    static constexpr int BW = TILE_X + 2 * XOFF;
+    static constexpr int PLANE = HY * BW;
+    // shared index of the thread's own column in a halo plane
+    static __device__ __forceinline__ int center() {
+        return ((threadIdx.x / TILE_X) + 1) * BW + (threadIdx.x % TILE_X) + XOFF;
+    }
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Waits for the chunk of buffer b; gives up after MBAR_TIMEOUT_NS and raises
+// the handle's error flag (the grid barrier then ends the kernel).
+#define MBAR_TIMEOUT_NS 2000000000ull
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, GridBarrier *gb) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*(volatile int *)&gb->error) return false;
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > MBAR_TIMEOUT_NS) {
+            atomicExch(&gb->error, 1);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Box loads of one array for planes [k0, k0 + CHN) of the tile at (x0, y0).
+template <typename V, int CHN>
+__device__ __forceinline__ void tma_halo(V *dst, const CUtensorMap *map, int x0, int y0, int k0,
+                                         uint64_t *bar) {
+    tma_load_3d(dst, map, x0 - Halo<V>::XOFF, y0 - 1, k0, bar);
+}
+template <typename V, int CHN>
+__device__ __forceinline__ void tma_own(V *dst, const CUtensorMap *map, int x0, int y0, int k0,
+                                        uint64_t *bar) {
+    tma_load_3d(dst, map, x0, y0, k0, bar);
+}
+template <typename V, int CHN>
+constexpr unsigned halo_bytes() {
+    return (unsigned)(CHN * Halo<V>::PLANE * sizeof(V));
+}
+template <typename V, int CHN>
+constexpr unsigned own_bytes() {
+    return (unsigned)(CHN * OWN_PLANE * sizeof(V));
+}
+
+// Block-uniform state of the two staging buffers: mbarriers and the parity
+// each buffer's next completion will have.
+struct StageBars {
+    uint64_t *bar;      // bar[0], bar[1] in shared memory
+    unsigned parity;    // bit b: expected parity of buffer b
+    GridBarrier *gb;
+    __device__ __forceinline__ bool wait(int b) {
+        const bool ok = mbar_wait(bar + b, (parity >> b) & 1u, gb);
+        parity ^= 1u << b;
+        return ok;
+    }
+};

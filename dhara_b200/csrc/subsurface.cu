@@ -18,6 +18,7 @@
 // w = 1/dx^2, 1/dy^2, 1/dz^2,  D = Ss theta/(phi dt) + C/dt, which is the
 // reference's DIA row (subsurface.cu:83-102) rearranged.
 #include "device_common.cuh"
+#include "staging.cuh"
 
 #include <cstdio>
 
@@ -251,157 +252,370 @@ struct StencilW {
     T cx, cy, cz;
 };
 
-// Forward Thomas step for the column tridiagonal preconditioner.
+// Planes per staged chunk of the inner phases and of the FP64 outer residual.
 template <typename T>
-__device__ __forceinline__ void thomas_fwd(T rk, T a, T c, T bd, T &cprev, T &dprev, T *s_c, int k,
-                                           T *zg) {
-    const T inv = T(1) / (bd - a * cprev);
-    const T cp = c * inv;
-    const T dp = (rk - a * dprev) * inv;
-    s_c[k * TILE_THREADS + threadIdx.x] = cp;
-    *zg = dp;
-    cprev = cp;
-    dprev = dp;
-}
+struct Chunk {
+    static constexpr int inner = sizeof(T) == 4 ? CHUNK_F32 : CHUNK_F64;
+};
 
+// Bytes of one staging buffer of each phase (the kernel reserves two buffers
+// of the largest).
 template <typename T>
-__device__ __forceinline__ double thomas_bwd(const ColumnRef &cr, const T *s_c, T *z, const T *r) {
-    T zn = T(0);
-    double rz = 0.0;
-    long long g = cr.g0 + (long long)(cr.nz - 1) * cr.sxy;
-    for (int k = cr.nz - 1; k >= 0; --k, g -= cr.sxy) {
-        const T zk = z[g] - s_c[k * TILE_THREADS + threadIdx.x] * zn;
-        z[g] = zk;
-        zn = zk;
-        rz += (double)r[g] * (double)zk;
+struct StageSize {
+    static constexpr int C = Chunk<T>::inner;
+    // phase A: z, p_old, K (halo); D (own)
+    static constexpr size_t A = 3 * (size_t)halo_bytes<T, C>() + own_bytes<T, C>();
+    // phase B: p, q, d, r, 1/den, a/den (own)
+    static constexpr size_t B = 6 * (size_t)own_bytes<T, C>();
+    // phase R: x, K64 (halo); D64, b (own), all FP64
+    static constexpr size_t R = 2 * (size_t)halo_bytes<double, CH_R>() + 2 * (size_t)own_bytes<double, CH_R>();
+    static constexpr size_t buffer() { return A > B ? (A > R ? A : R) : (B > R ? B : R); }
+    static constexpr size_t bytes() { return 2 * buffer(); }
+};
+
+// Chunked march over a tile's planes: thread 0 arms and issues chunk st into
+// buffer st & 1 (issue(st, b)); every thread waits for the chunk and computes
+// its planes (plane(b, pl, k)).  With NEXT, the last plane of a chunk also reads
+// the first plane of the next chunk (the z-neighbour of a stencil), which is
+// awaited first.  A buffer is refilled with chunk st + 2 once all threads are
+// done with it; when the tile is done, issue_next() starts the block's next
+// tile so its first chunks stream in during this tile's epilogue.
+template <int CHN, bool NEXT, typename Issue, typename PlaneFn, typename NextFn>
+__device__ __forceinline__ void march(int nz, StageBars &sb, bool prefetched, Issue issue, PlaneFn plane,
+                                      NextFn issue_next) {
+    const int nst = (nz + CHN - 1) / CHN;
+    if (threadIdx.x == 0 && !prefetched) {
+        issue(0, 0);
+        if (nst > 1) issue(1, 1);
     }
-    return rz;
+    bool next_ready = false;
+    for (int st = 0; st < nst; ++st) {
+        const int b = st & 1;
+        if (!next_ready) sb.wait(b);
+        next_ready = false;
+        for (int pl = 0; pl < CHN; ++pl) {
+            const int k = st * CHN + pl;
+            if (k >= nz) break;
+            if (NEXT && pl == CHN - 1 && k + 1 < nz) {
+                sb.wait(b ^ 1);
+                next_ready = true;
+            }
+            plane(b, pl, k);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && st + 2 < nst) issue(st + 2, b);
+    }
+    if (threadIdx.x == 0) issue_next();
 }
 
-// Lateral face conductivities and neighbour values of vector v at cell g.
-template <typename T, typename V, typename Get>
-__device__ __forceinline__ void lateral(const ColumnRef &cr, const T *__restrict__ K, long long g,
-                                        T Kc, Get get, T &kw, T &ke, T &ks, T &kn, V &vw, V &ve,
-                                        V &vs, V &vn) {
-    kw = ke = ks = kn = T(0);
-    vw = ve = vs = vn = V(0);
-    if (cr.i > 0) { kw = T(0.5) * (Kc + __ldg(K + g - 1)); vw = get(g - 1); }
-    if (cr.i < cr.nx - 1) { ke = T(0.5) * (Kc + __ldg(K + g + 1)); ve = get(g + 1); }
-    if (cr.j > 0) { ks = T(0.5) * (Kc + __ldg(K + g - cr.nx)); vs = get(g - cr.nx); }
-    if (cr.j < cr.ny - 1) { kn = T(0.5) * (Kc + __ldg(K + g + cr.nx)); vn = get(g + cr.nx); }
+// The column preconditioner M is the z-coupled (tridiagonal) part of A:
+// b_k = D_k + sum_f w_f k_f, a_k = -w_z kd_k, c_k = -w_z ku_k.  It is factored
+// once per outer cycle (phase R) by the Thomas algorithm,
+//   den_k = b_k - a_k c'_{k-1},  c'_k = c_k / den_k,
+// and the factors 1/den, e = a/den and c' are stored per cell, so applying M^-1
+// in the inner iterations is two FMA recurrences:
+//   forward  d'_k = r_k / den_k - e_k d'_{k-1},  backward z_k = d'_k - c'_k z_{k+1}.
+// With M = L D L^T (D = den), r^T M^-1 r = sum_k den_k d'_k^2 is accumulated in
+// the forward sweep.  d' lives in shared memory when T is float (DSMEM), else
+// in the z array itself.
+template <typename T, bool DSMEM>
+__device__ __forceinline__ void put_dprime(T dp, T *s_d, int k, T *__restrict__ zg) {
+    if (DSMEM) s_d[k * TILE_THREADS + threadIdx.x] = dp;
+    else *zg = dp;
 }
 
-// Phase R: FP64 residual with the FP64 coefficients, its cast to T, the
-// column solve with the T coefficients of the inner operator (the same
-// rounding as the stored K, D), and partial sums v = {||r||^2, ||b||^2, r.z}.
+template <typename T, bool DSMEM>
+__device__ __forceinline__ void back_sweep(const ColumnRef &cr, const T *s_d, const T *__restrict__ fc,
+                                           T *__restrict__ z) {
+    T zn = T(0);
+    for (int k0 = cr.nz - 1; k0 >= 0; k0 -= 8) {
+        T cl[8], dl[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int k = k0 - q;
+            if (k >= 0) {
+                const long long g = cr.g0 + (long long)k * cr.sxy;
+                cl[q] = fc[g];
+                dl[q] = DSMEM ? s_d[k * TILE_THREADS + threadIdx.x] : z[g];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int k = k0 - q;
+            if (k >= 0) {
+                const T zk = dl[q] - cl[q] * zn;
+                z[cr.g0 + (long long)k * cr.sxy] = zk;
+                zn = zk;
+            }
+        }
+    }
+}
+
 template <typename T>
-__device__ void phase_R(const DevPtrs &P, const ColumnRef &cr, const StencilW<T> &w, T *s_c,
-                        double (&v)[3]) {
-    const double *__restrict__ K = P.K64;
-    const double *__restrict__ Dg = P.D64;
-    T *r = (T *)P.r, *z = (T *)P.z;
-    const double *x = P.x;
-    const int nz = cr.nz;
-    long long g = cr.g0;
-    double x_up = 0.0, x_c = x[g], x_dn = 0.0;
-    double K_up = 0.0, K_c = __ldg(K + g), K_dn = 0.0;
-    T cprev = T(0), dprev = T(0);
+__device__ __forceinline__ T recip(T x);
+template <>
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
+template <>
+__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
+
+// Face masks of a column: 1 where the face is interior, 0 on a domain face.
+struct Masks {
+    double w, e, s, n;
+};
+__device__ __forceinline__ Masks masks_of(const ColumnRef &cr) {
+    Masks m;
+    m.w = cr.i > 0 ? 1.0 : 0.0;
+    m.e = cr.i < cr.nx - 1 ? 1.0 : 0.0;
+    m.s = cr.j > 0 ? 1.0 : 0.0;
+    m.n = cr.j < cr.ny - 1 ? 1.0 : 0.0;
+    return m;
+}
+
+// Chunk issue of each phase for tile `tile` (thread 0 only): arms buffer b's
+// mbarrier with the chunk's bytes and starts one TMA box load per array.
+template <typename T>
+__device__ __forceinline__ void issue_R(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
+                                        StageBars &sb) {
+    constexpr int CHN = CH_R;
+    constexpr unsigned HB = halo_bytes<double, CHN>(), OB = own_bytes<double, CHN>();
+    const TileDesc td = P.tiles[tile];
+    const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
+    unsigned char *B = stage + b * StageSize<T>::buffer();
+    const int k0 = st * CHN;
+    mbar_expect_tx(sb.bar + b, 2 * HB + 2 * OB);
+    tma_halo<double, CHN>((double *)B, maps + MAP_X64_H, td.x0, td.y0, k0, sb.bar + b);
+    tma_halo<double, CHN>((double *)(B + HB), maps + MAP_K64_H, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<double, CHN>((double *)(B + 2 * HB), maps + MAP_D64_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<double, CHN>((double *)(B + 2 * HB + OB), maps + MAP_B_O, td.x0, td.y0, k0, sb.bar + b);
+}
+
+template <typename T>
+__device__ __forceinline__ void issue_A(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
+                                        StageBars &sb, bool first, int parity_old) {
+    constexpr int CHN = Chunk<T>::inner;
+    constexpr unsigned HB = halo_bytes<T, CHN>(), OB = own_bytes<T, CHN>();
+    const TileDesc td = P.tiles[tile];
+    const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
+    unsigned char *B = stage + b * StageSize<T>::buffer();
+    const int k0 = st * CHN;
+    mbar_expect_tx(sb.bar + b, (first ? 2 : 3) * HB + OB);
+    tma_halo<T, CHN>((T *)B, maps + MAP_Z_H, td.x0, td.y0, k0, sb.bar + b);
+    if (!first)
+        tma_halo<T, CHN>((T *)(B + HB), maps + (parity_old ? MAP_P1_H : MAP_P0_H), td.x0, td.y0, k0, sb.bar + b);
+    tma_halo<T, CHN>((T *)(B + 2 * HB), maps + MAP_K_H, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + 3 * HB), maps + MAP_D_O, td.x0, td.y0, k0, sb.bar + b);
+}
+
+template <typename T>
+__device__ __forceinline__ void issue_B(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
+                                        StageBars &sb, bool first, int parity_p) {
+    constexpr int CHN = Chunk<T>::inner;
+    constexpr unsigned OB = own_bytes<T, CHN>();
+    const TileDesc td = P.tiles[tile];
+    const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
+    unsigned char *B = stage + b * StageSize<T>::buffer();
+    const int k0 = st * CHN;
+    mbar_expect_tx(sb.bar + b, (first ? 5 : 6) * OB);
+    tma_own<T, CHN>((T *)B, maps + (parity_p ? MAP_P1_O : MAP_P0_O), td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + OB), maps + MAP_Q_O, td.x0, td.y0, k0, sb.bar + b);
+    if (!first) tma_own<T, CHN>((T *)(B + 2 * OB), maps + MAP_DD_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + 3 * OB), maps + MAP_R_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + 4 * OB), maps + MAP_INV_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + 5 * OB), maps + MAP_E_O, td.x0, td.y0, k0, sb.bar + b);
+}
+
+// Issues chunks 0 and 1 of a tile (the prefetch of the block's next tile).
+template <int CHN, typename Issue>
+__device__ __forceinline__ void issue_head(int nz, Issue issue) {
+    issue(0, 0);
+    if (nz > CHN) issue(1, 1);
+}
+
+// ---- phase R: outer FP64 residual and the preconditioner factors -------------
+// r = b - A x with the FP64 coefficients, r_T = (T) r; the column factors of M
+// from the inner operator's T coefficients (the same rounding as the stored
+// K, D) are stored; z = M^-1 r_T; v = {||r||^2, ||b||^2, r.z}.
+// Staged: x, K64 (halo), D64, b (own).
+template <typename T, bool DSMEM>
+__device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetched, const ColumnRef &cr,
+                        const StencilW<T> &w, T *s_d, unsigned char *stage, StageBars &sb, double (&v)[3]) {
+    constexpr int CHN = CH_R;
+    typedef Halo<double> H;
+    constexpr unsigned HB = halo_bytes<double, CHN>(), OB = own_bytes<double, CHN>();
+    T *__restrict__ r = (T *)P.r;
+    T *__restrict__ z = (T *)P.z;
+    T *__restrict__ finv = (T *)P.finv;
+    T *__restrict__ fe = (T *)P.fe;
+    T *__restrict__ fc = (T *)P.fc;
+    const size_t BUF = StageSize<T>::buffer();
+    auto buf = [&](int b) { return stage + b * BUF; };
+    auto issue = [&](int st, int b) { issue_R<T>(P, tile, st, b, stage, sb); };
+    auto issue_next = [&]() {
+        if (tile_next < P.ntiles)
+            issue_head<CHN>(P.dom[P.tiles[tile_next].dom].nz,
+                            [&](int st, int b) { issue_R<T>(P, tile_next, st, b, stage, sb); });
+    };
+    const int nz = cr.nz, hc = H::center(), oc = threadIdx.x;
+    const Masks M = masks_of(cr);
     const double cx = (double)w.cx, cy = (double)w.cy, cz = (double)w.cz;
-    for (int k = 0; k < nz; ++k, g += cr.sxy) {
-        if (k + 1 < nz) { x_dn = x[g + cr.sxy]; K_dn = __ldg(K + g + cr.sxy); }
-        else { x_dn = 0.0; K_dn = 0.0; }
-        const double kd = (k > 0) ? 0.5 * (K_c + K_up) : 0.0;
-        const double ku = (k < nz - 1) ? 0.5 * (K_c + K_dn) : 0.0;
-        double kw, ke, ks, kn, xw, xe, xs, xn;
-        lateral<double, double>(cr, K, g, K_c, [&](long long q) { return x[q]; }, kw, ke, ks, kn, xw, xe,
-                                xs, xn);
-        const double Dk = __ldg(Dg + g);
-        const double Ax = Dk * x_c + cx * (kw * (x_c - xw) + ke * (x_c - xe)) +
-                          cy * (ks * (x_c - xs) + kn * (x_c - xn)) +
-                          cz * (kd * (x_c - x_up) + ku * (x_c - x_dn));
-        const double bk = __ldg(P.b + g);
+    double x_up = 0.0, K_up = 0.0;
+    T cprev = T(0), dprev = T(0);
+    auto plane = [&](int b, int pl, int k) {
+        if (!cr.valid) return;
+        const double *sx = (const double *)buf(b) + pl * H::PLANE;
+        const double *sK = (const double *)(buf(b) + HB) + pl * H::PLANE;
+        const double *sD = (const double *)(buf(b) + 2 * HB) + pl * OWN_PLANE;
+        const double *sb_ = (const double *)(buf(b) + 2 * HB + OB) + pl * OWN_PLANE;
+        const double xc = sx[hc], Kc = sK[hc];
+        double x_dn = 0.0, K_dn = 0.0;
+        if (k + 1 < nz) {
+            if (pl + 1 < CHN) { x_dn = sx[H::PLANE + hc]; K_dn = sK[H::PLANE + hc]; }
+            else { x_dn = ((const double *)buf(b ^ 1))[hc]; K_dn = ((const double *)(buf(b ^ 1) + HB))[hc]; }
+        }
+        const double mu = k > 0 ? 1.0 : 0.0, md = k < nz - 1 ? 1.0 : 0.0;
+        const double Kw = sK[hc - 1], Ke = sK[hc + 1], Ks = sK[hc - H::BW], Kn = sK[hc + H::BW];
+        const double kd = mu * 0.5 * (Kc + K_up), ku = md * 0.5 * (Kc + K_dn);
+        const double kw = M.w * 0.5 * (Kc + Kw), ke = M.e * 0.5 * (Kc + Ke);
+        const double ks = M.s * 0.5 * (Kc + Ks), kn = M.n * 0.5 * (Kc + Kn);
+        const double Dk = sD[oc], bk = sb_[oc];
+        const double Ax = Dk * xc + cx * (kw * (xc - sx[hc - 1]) + ke * (xc - sx[hc + 1])) +
+                          cy * (ks * (xc - sx[hc - H::BW]) + kn * (xc - sx[hc + H::BW])) +
+                          cz * (kd * (xc - x_up) + ku * (xc - x_dn));
         const double rk = bk - Ax;
         v[0] += rk * rk;
         v[1] += bk * bk;
         const T rT = (T)rk;
+        const long long g = cr.g0 + (long long)k * cr.sxy;
         r[g] = rT;
-        // inner-operator coefficients: T-rounded cell values, T arithmetic
-        const T Kt = (T)K_c;
-        const T kdT = (k > 0) ? T(0.5) * (Kt + (T)K_up) : T(0);
-        const T kuT = (k < nz - 1) ? T(0.5) * (Kt + (T)K_dn) : T(0);
-        const T kwT = cr.i > 0 ? T(0.5) * (Kt + (T)__ldg(K + g - 1)) : T(0);
-        const T keT = cr.i < cr.nx - 1 ? T(0.5) * (Kt + (T)__ldg(K + g + 1)) : T(0);
-        const T ksT = cr.j > 0 ? T(0.5) * (Kt + (T)__ldg(K + g - cr.nx)) : T(0);
-        const T knT = cr.j < cr.ny - 1 ? T(0.5) * (Kt + (T)__ldg(K + g + cr.nx)) : T(0);
+        const T Kt = (T)Kc;
+        const T kdT = T(mu) * (T(0.5) * (Kt + (T)K_up)), kuT = T(md) * (T(0.5) * (Kt + (T)K_dn));
+        const T kwT = T(M.w) * (T(0.5) * (Kt + (T)Kw)), keT = T(M.e) * (T(0.5) * (Kt + (T)Ke));
+        const T ksT = T(M.s) * (T(0.5) * (Kt + (T)Ks)), knT = T(M.n) * (T(0.5) * (Kt + (T)Kn));
         const T bd = (T)Dk + w.cx * (kwT + keT) + w.cy * (ksT + knT) + w.cz * (kdT + kuT);
-        thomas_fwd<T>(rT, -w.cz * kdT, -w.cz * kuT, bd, cprev, dprev, s_c, k, z + g);
-        x_up = x_c; x_c = x_dn; K_up = K_c; K_c = K_dn;
-    }
-    v[2] += thomas_bwd<T>(cr, s_c, z, r);
+        const T a = -w.cz * kdT, c = -w.cz * kuT;
+        const T den = bd - a * cprev;
+        const T inv = recip(den);
+        const T cp = c * inv, e = a * inv;
+        const T dp = rT * inv - e * dprev;
+        finv[g] = inv;
+        fe[g] = e;
+        fc[g] = cp;
+        put_dprime<T, DSMEM>(dp, s_d, k, z + g);
+        v[2] += (double)den * (double)dp * (double)dp;
+        cprev = cp;
+        dprev = dp;
+        x_up = xc;
+        K_up = Kc;
+    };
+    march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next);
+    if (cr.valid) back_sweep<T, DSMEM>(cr, s_d, fc, z);
 }
 
-// Phase A: p_new = z + beta p_old (recomputed at the halo, double-buffered p),
-// partial p.Ap.
+// ---- phase A: direction and q = A p ------------------------------------------
+// p_new = z + beta p_old (formed at the lateral neighbours from the staged z and
+// p_old; p is double buffered), q = A p_new, v = {p.q}.
+// Staged: z, p_old, K (halo), D (own).
 template <typename T>
-__device__ void phase_A(const DevPtrs &P, const ColumnRef &cr, const StencilW<T> &w, T beta,
-                        bool first, const T *pold, T *pnew, double (&v)[1]) {
-    const T *__restrict__ K = (const T *)P.K;
-    const T *__restrict__ Dg = (const T *)P.D;
-    const T *z = (const T *)P.z;
-    const int nz = cr.nz;
-    auto pv = [&](long long q) -> T { return first ? z[q] : z[q] + beta * pold[q]; };
-    long long g = cr.g0;
-    T p_up = T(0), p_c = pv(g), p_dn = T(0);
-    T K_up = T(0), K_c = __ldg(K + g), K_dn = T(0);
-    for (int k = 0; k < nz; ++k, g += cr.sxy) {
-        if (k + 1 < nz) { p_dn = pv(g + cr.sxy); K_dn = __ldg(K + g + cr.sxy); }
-        else { p_dn = T(0); K_dn = T(0); }
-        const T kd = (k > 0) ? T(0.5) * (K_c + K_up) : T(0);
-        const T ku = (k < nz - 1) ? T(0.5) * (K_c + K_dn) : T(0);
-        T kw, ke, ks, kn, pw, pe, ps, pn;
-        lateral<T, T>(cr, K, g, K_c, pv, kw, ke, ks, kn, pw, pe, ps, pn);
-        const T Ap = __ldg(Dg + g) * p_c + w.cx * (kw * (p_c - pw) + ke * (p_c - pe)) +
-                     w.cy * (ks * (p_c - ps) + kn * (p_c - pn)) +
-                     w.cz * (kd * (p_c - p_up) + ku * (p_c - p_dn));
-        v[0] += (double)p_c * (double)Ap;
-        pnew[g] = p_c;
-        p_up = p_c; p_c = p_dn; K_up = K_c; K_c = K_dn;
-    }
+__device__ void phase_A(const DevPtrs &P, int tile, int tile_next, bool prefetched, bool first_next,
+                        int parity_next, const ColumnRef &cr, const StencilW<T> &w, T beta, bool first,
+                        int parity_old, T *__restrict__ pnew, unsigned char *stage, StageBars &sb,
+                        double (&v)[1]) {
+    constexpr int CHN = Chunk<T>::inner;
+    typedef Halo<T> H;
+    constexpr unsigned HB = halo_bytes<T, CHN>();
+    T *__restrict__ q = (T *)P.q;
+    const size_t BUF = StageSize<T>::buffer();
+    auto buf = [&](int b) { return stage + b * BUF; };
+    auto issue = [&](int st, int b) { issue_A<T>(P, tile, st, b, stage, sb, first, parity_old); };
+    auto issue_next = [&]() {
+        if (tile_next < P.ntiles)
+            issue_head<CHN>(P.dom[P.tiles[tile_next].dom].nz, [&](int st, int b) {
+                issue_A<T>(P, tile_next, st, b, stage, sb, first_next, parity_next);
+            });
+    };
+    const int nz = cr.nz, hc = H::center(), oc = threadIdx.x;
+    const Masks M = masks_of(cr);
+    const T mW = (T)M.w, mE = (T)M.e, mS = (T)M.s, mN = (T)M.n;
+    const T bt = first ? T(0) : beta;
+    T p_up = T(0), K_up = T(0);
+    auto plane = [&](int b, int pl, int k) {
+        if (!cr.valid) return;
+        const T *sz = (const T *)buf(b) + pl * H::PLANE;
+        const T *sq = (const T *)(buf(b) + HB) + pl * H::PLANE;
+        const T *sK = (const T *)(buf(b) + 2 * HB) + pl * H::PLANE;
+        const T *sD = (const T *)(buf(b) + 3 * HB) + pl * OWN_PLANE;
+        auto pv = [&](const T *zz, const T *qq, int o) { return first ? zz[o] : zz[o] + bt * qq[o]; };
+        const T pc = pv(sz, sq, hc);
+        T p_dn = T(0), K_dn = T(0);
+        if (k + 1 < nz) {
+            if (pl + 1 < CHN) { p_dn = pv(sz + H::PLANE, sq + H::PLANE, hc); K_dn = sK[H::PLANE + hc]; }
+            else {
+                const T *nz_ = (const T *)buf(b ^ 1), *nq = (const T *)(buf(b ^ 1) + HB);
+                p_dn = pv(nz_, nq, hc);
+                K_dn = ((const T *)(buf(b ^ 1) + 2 * HB))[hc];
+            }
+        }
+        const T Kc = sK[hc];
+        const T mu = k > 0 ? T(1) : T(0), md = k < nz - 1 ? T(1) : T(0);
+        const T kd = mu * (T(0.5) * (Kc + K_up)), ku = md * (T(0.5) * (Kc + K_dn));
+        const T kw = mW * (T(0.5) * (Kc + sK[hc - 1])), ke = mE * (T(0.5) * (Kc + sK[hc + 1]));
+        const T ks = mS * (T(0.5) * (Kc + sK[hc - H::BW])), kn = mN * (T(0.5) * (Kc + sK[hc + H::BW]));
+        const T Ap = sD[oc] * pc + w.cx * (kw * (pc - pv(sz, sq, hc - 1)) + ke * (pc - pv(sz, sq, hc + 1))) +
+                     w.cy * (ks * (pc - pv(sz, sq, hc - H::BW)) + kn * (pc - pv(sz, sq, hc + H::BW))) +
+                     w.cz * (kd * (pc - p_up) + ku * (pc - p_dn));
+        v[0] += (double)pc * (double)Ap;
+        const long long g = cr.g0 + (long long)k * cr.sxy;
+        pnew[g] = pc;
+        q[g] = Ap;
+        p_up = pc;
+        K_up = Kc;
+    };
+    march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next);
 }
 
-// Phase B: d += alpha p, r -= alpha A p (A p recomputed), z = M^-1 r,
-// partials {||r||^2, r.z}.
-template <typename T>
-__device__ void phase_B(const DevPtrs &P, const ColumnRef &cr, const StencilW<T> &w, T alpha,
-                        bool first, const T *p, T *s_c, double (&v)[2]) {
-    const T *__restrict__ K = (const T *)P.K;
-    const T *__restrict__ Dg = (const T *)P.D;
-    T *r = (T *)P.r, *z = (T *)P.z, *d = (T *)P.d;
-    const int nz = cr.nz;
-    long long g = cr.g0;
-    T p_up = T(0), p_c = p[g], p_dn = T(0);
-    T K_up = T(0), K_c = __ldg(K + g), K_dn = T(0);
-    T cprev = T(0), dprev = T(0);
-    for (int k = 0; k < nz; ++k, g += cr.sxy) {
-        if (k + 1 < nz) { p_dn = p[g + cr.sxy]; K_dn = __ldg(K + g + cr.sxy); }
-        else { p_dn = T(0); K_dn = T(0); }
-        const T kd = (k > 0) ? T(0.5) * (K_c + K_up) : T(0);
-        const T ku = (k < nz - 1) ? T(0.5) * (K_c + K_dn) : T(0);
-        T kw, ke, ks, kn, pw, pe, ps, pn;
-        lateral<T, T>(cr, K, g, K_c, [&](long long q) { return p[q]; }, kw, ke, ks, kn, pw, pe, ps, pn);
-        const T Dk = __ldg(Dg + g);
-        const T Ap = Dk * p_c + w.cx * (kw * (p_c - pw) + ke * (p_c - pe)) +
-                     w.cy * (ks * (p_c - ps) + kn * (p_c - pn)) +
-                     w.cz * (kd * (p_c - p_up) + ku * (p_c - p_dn));
-        d[g] = first ? alpha * p_c : d[g] + alpha * p_c;
-        const T rk = r[g] - alpha * Ap;
+// ---- phase B: update, residual, preconditioner --------------------------------
+// d += alpha p, r -= alpha q, z = M^-1 r with the stored factors;
+// v = {||r||^2, r.z}.  Column-local: staged p, q, d, r, 1/den, a/den (own).
+template <typename T, bool DSMEM>
+__device__ void phase_B(const DevPtrs &P, int tile, int tile_next, bool prefetched, bool first_next,
+                        int parity_next, const ColumnRef &cr, T alpha, bool first, int parity_p, T *s_d,
+                        unsigned char *stage, StageBars &sb, double (&v)[2]) {
+    constexpr int CHN = Chunk<T>::inner;
+    constexpr unsigned OB = own_bytes<T, CHN>();
+    T *__restrict__ r = (T *)P.r;
+    T *__restrict__ z = (T *)P.z;
+    T *__restrict__ d = (T *)P.d;
+    const T *__restrict__ fc = (const T *)P.fc;
+    const size_t BUF = StageSize<T>::buffer();
+    auto buf = [&](int b) { return stage + b * BUF; };
+    auto issue = [&](int st, int b) { issue_B<T>(P, tile, st, b, stage, sb, first, parity_p); };
+    auto issue_next = [&]() {
+        if (tile_next < P.ntiles)
+            issue_head<CHN>(P.dom[P.tiles[tile_next].dom].nz, [&](int st, int b) {
+                issue_B<T>(P, tile_next, st, b, stage, sb, first_next, parity_next);
+            });
+    };
+    const int nz = cr.nz, oc = threadIdx.x;
+    T dprev = T(0);
+    auto plane = [&](int b, int pl, int k) {
+        if (!cr.valid) return;
+        const T *B = (const T *)buf(b) + pl * OWN_PLANE + oc;
+        constexpr int S = CHN * OWN_PLANE;
+        const T pc = B[0], qc = B[S], dold = first ? T(0) : B[2 * S], rold = B[3 * S];
+        const T inv = B[4 * S], e = B[5 * S];
+        const long long g = cr.g0 + (long long)k * cr.sxy;
+        d[g] = dold + alpha * pc;
+        const T rk = rold - alpha * qc;
         r[g] = rk;
         v[0] += (double)rk * (double)rk;
-        const T bd = Dk + w.cx * (kw + ke) + w.cy * (ks + kn) + w.cz * (kd + ku);
-        thomas_fwd<T>(rk, -w.cz * kd, -w.cz * ku, bd, cprev, dprev, s_c, k, z + g);
-        p_up = p_c; p_c = p_dn; K_up = K_c; K_c = K_dn;
-    }
-    v[1] += thomas_bwd<T>(cr, s_c, z, r);
+        const T dp = rk * inv - e * dprev;
+        put_dprime<T, DSMEM>(dp, s_d, k, z + g);
+        v[1] += (double)dp * (double)dp / (double)inv;
+        dprev = dp;
+    };
+    march<CHN, false>(nz, sb, prefetched, issue, plane, issue_next);
+    (void)OB;
+    if (cr.valid) back_sweep<T, DSMEM>(cr, s_d, fc, z);
 }
 
 __device__ __forceinline__ void finalize_R(const DevPtrs &P, int dom, const double (&v)[3]) {
@@ -439,40 +653,75 @@ __device__ __forceinline__ void stop_inner(const DevPtrs &P, KrylovCtrl &c) {
 
 template <typename T>
 __global__ void __launch_bounds__(TILE_THREADS) k_krylov(DevPtrs P) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *s_c = reinterpret_cast<T *>(smem_raw);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    constexpr bool DSMEM = sizeof(T) == 4;
+    // dynamic shared memory: [d' of the column solves (float only)][two staging
+    // buffers], the staging buffers 128-byte aligned for the TMA
+    unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    T *s_d = reinterpret_cast<T *>(base);
+    const size_t dprime_bytes = DSMEM ? (size_t)P.smem_nz * TILE_THREADS * sizeof(T) : 0;
+    unsigned char *stage_raw = base + ((dprime_bytes + 127) & ~(size_t)127);
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    StageBars sb{s_bar, 0u, P.barrier};
+    // next tile of this block with an active domain (stride gridDim.x)
+    auto next_outer = [&](int t) {
+        while (t < P.ntiles && !ldcg(&P.kctrl[P.tiles[t].dom].active)) t += gridDim.x;
+        return t;
+    };
+    auto next_inner = [&](int t) {
+        while (t < P.ntiles && !ldcg(&P.kctrl[P.tiles[t].dom].inner_active)) t += gridDim.x;
+        return t;
+    };
+    auto weights = [&](int dom) {
+        const DomainDesc &D = P.dom[dom];
+        return StencilW<T>{(T)(1.0 / (D.dx * D.dx)), (T)(1.0 / (D.dy * D.dy)), (T)(1.0 / (D.dz * D.dz))};
+    };
     for (;;) {
         // ---- R: outer residual
-        for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-            const int dom = P.tiles[t].dom;
-            if (!ldcg(&P.kctrl[dom].active)) continue;
-            const ColumnRef cr = column_of(P, t);
-            const DomainDesc &D = P.dom[dom];
-            const StencilW<T> w = {(T)(1.0 / (D.dx * D.dx)), (T)(1.0 / (D.dy * D.dy)),
-                                   (T)(1.0 / (D.dz * D.dz))};
-            double v[3] = {0.0, 0.0, 0.0};
-            if (cr.valid) phase_R<T>(P, cr, w, s_c, v);
-            if (domain_reduce<3>(P, t, dom, 0, v) && threadIdx.x == 0) finalize_R(P, dom, v);
+        {
+            bool pre = false;
+            for (int t = next_outer(blockIdx.x); t < P.ntiles;) {
+                const int tn = next_outer(t + gridDim.x);
+                const int dom = P.tiles[t].dom;
+                const ColumnRef cr = column_of(P, t);
+                double v[3] = {0.0, 0.0, 0.0};
+                phase_R<T, DSMEM>(P, t, tn, pre, cr, weights(dom), s_d, stage_raw, sb, v);
+                pre = tn < P.ntiles;
+                if (domain_reduce<3>(P, t, dom, 0, v) && threadIdx.x == 0) finalize_R(P, dom, v);
+                t = tn;
+            }
         }
         if (!grid_sync(P.barrier)) return;
         if (ldcg(&P.gctrl->n_active) == 0) break;
         // ---- inner PCG
         while (ldcg(&P.gctrl->n_inner_active) > 0) {
-            for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+            bool pre = false;
+            for (int t = next_inner(blockIdx.x); t < P.ntiles;) {
+                const int tn = next_inner(t + gridDim.x);
                 const int dom = P.tiles[t].dom;
                 const KrylovCtrl *kc = &P.kctrl[dom];
-                if (!ldcg(&kc->inner_active)) continue;
                 const ColumnRef cr = column_of(P, t);
-                const DomainDesc &D = P.dom[dom];
-                const StencilW<T> w = {(T)(1.0 / (D.dx * D.dx)), (T)(1.0 / (D.dy * D.dy)),
-                                       (T)(1.0 / (D.dz * D.dz))};
                 const int parity = ldcg(&kc->parity);
                 const bool first = ldcg(&kc->first_inner) != 0;
                 const T beta = (T)ldcg(&kc->beta);
-                const T *pold = (const T *)(parity ? P.p1 : P.p0);
+                bool first_n = false;
+                int parity_n = 0;
+                if (tn < P.ntiles) {
+                    const KrylovCtrl *kn = &P.kctrl[P.tiles[tn].dom];
+                    first_n = ldcg(&kn->first_inner) != 0;
+                    parity_n = ldcg(&kn->parity);
+                }
                 T *pnew = (T *)(parity ? P.p0 : P.p1);
                 double v[1] = {0.0};
-                if (cr.valid) phase_A<T>(P, cr, w, beta, first, pold, pnew, v);
+                phase_A<T>(P, t, tn, pre, first_n, parity_n, cr, weights(dom), beta, first, parity, pnew,
+                           stage_raw, sb, v);
+                pre = tn < P.ntiles;
                 if (domain_reduce<1>(P, t, dom, 0, v) && threadIdx.x == 0) {
                     KrylovCtrl &c = P.kctrl[dom];
                     c.pAp = v[0];
@@ -480,22 +729,30 @@ __global__ void __launch_bounds__(TILE_THREADS) k_krylov(DevPtrs P) {
                     c.parity ^= 1;
                     if (!(v[0] > 0.0) || isinf(v[0])) stop_inner(P, c);
                 }
+                t = tn;
             }
             if (!grid_sync(P.barrier)) return;
-            for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+            pre = false;
+            for (int t = next_inner(blockIdx.x); t < P.ntiles;) {
+                const int tn = next_inner(t + gridDim.x);
                 const int dom = P.tiles[t].dom;
                 const KrylovCtrl *kc = &P.kctrl[dom];
-                if (!ldcg(&kc->inner_active)) continue;
                 const ColumnRef cr = column_of(P, t);
                 const DomainDesc &D = P.dom[dom];
-                const StencilW<T> w = {(T)(1.0 / (D.dx * D.dx)), (T)(1.0 / (D.dy * D.dy)),
-                                       (T)(1.0 / (D.dz * D.dz))};
                 const int parity = ldcg(&kc->parity);
                 const bool first = ldcg(&kc->first_inner) != 0;
                 const T alpha = (T)ldcg(&kc->alpha);
-                const T *p = (const T *)(parity ? P.p1 : P.p0);
+                bool first_n = false;
+                int parity_n = 0;
+                if (tn < P.ntiles) {
+                    const KrylovCtrl *kn = &P.kctrl[P.tiles[tn].dom];
+                    first_n = ldcg(&kn->first_inner) != 0;
+                    parity_n = ldcg(&kn->parity);
+                }
                 double v[2] = {0.0, 0.0};
-                if (cr.valid) phase_B<T>(P, cr, w, alpha, first, p, s_c, v);
+                phase_B<T, DSMEM>(P, t, tn, pre, first_n, parity_n, cr, alpha, first, parity, s_d, stage_raw,
+                                  sb, v);
+                pre = tn < P.ntiles;
                 if (domain_reduce<2>(P, t, dom, 0, v) && threadIdx.x == 0) {
                     KrylovCtrl &c = P.kctrl[dom];
                     c.rr = v[0];
@@ -508,6 +765,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_krylov(DevPtrs P) {
                         c.total_iter >= D.krylov_maxiter || !(v[0] == v[0]) || !(v[1] == v[1]))
                         stop_inner(P, c);
                 }
+                t = tn;
             }
             if (!grid_sync(P.barrier)) return;
         }
@@ -518,9 +776,13 @@ __global__ void __launch_bounds__(TILE_THREADS) k_krylov(DevPtrs P) {
             if (!ldcg(&kc->active) || ldcg(&kc->first_inner)) continue;
             const ColumnRef cr = column_of(P, t);
             if (!cr.valid) continue;
-            const T *d = (const T *)P.d;
-            long long g = cr.g0;
-            for (int k = 0; k < cr.nz; ++k, g += cr.sxy) P.x[g] += (double)d[g];
+            const T *__restrict__ d = (const T *)P.d;
+            double *__restrict__ x = P.x;
+#pragma unroll 8
+            for (int k = 0; k < cr.nz; ++k) {
+                const long long g = cr.g0 + (long long)k * cr.sxy;
+                x[g] += (double)d[g];
+            }
         }
         if (!grid_sync(P.barrier)) return;
     }
@@ -734,7 +996,9 @@ cudaError_t configure_3d(LaunchCfg &L, int device, int ntiles) {
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e != cudaSuccess) return e;
     const size_t elt = L.mixed ? sizeof(float) : sizeof(double);
-    L.smem_3d = (int)(elt * (size_t)L.nz_max * TILE_THREADS);
+    const size_t dprime = L.mixed ? elt * (size_t)L.nz_max * TILE_THREADS : 0;
+    const size_t stage = L.mixed ? StageSize<float>::bytes() : StageSize<double>::bytes();
+    L.smem_3d = (int)(128 + ((dprime + 127) & ~(size_t)127) + stage);
     const void *fn = L.mixed ? (const void *)k_krylov<float> : (const void *)k_krylov<double>;
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_3d);
     if (e != cudaSuccess) return e;
