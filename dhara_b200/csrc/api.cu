@@ -360,6 +360,13 @@ int build_tensor_maps(dhara_handle *h) {
 
 }  // namespace
 
+// Lets the library's other translation units report through dhara_last_error
+// (not exported).
+__attribute__((visibility("hidden"))) int dhara_internal_fail(int code, const char *msg) {
+    g_err = msg;
+    return code;
+}
+
 // ====================================================================== ABI
 extern "C" {
 

@@ -238,6 +238,26 @@ int dhara_get_launch_count(dhara_handle *h, int64_t *count);
  * roofline figure divides by time), and the inner iterations they cover. */
 int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations);
 
+/* ---- allocation-free overland step ---------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they step (a host model that owns every GPU buffer, code
+ * running during CUDA stream capture, a loop that forbids allocation after
+ * start-up): one overland step of one domain -- the computation of
+ * dhara_overland_step -- on the caller's device arrays.  waterdepth is read
+ * as the depth before the step and overwritten with the depth after it;
+ * waterelev receives H = h + z after the solve; ztopo and mann are read.
+ * Uses nx, ny, dx, dy, dt, delta, hmin, K0, overland_tol, overland_maxiter of
+ * *p.  Work is queued on `stream` (a cudaStream_t; NULL = default stream).
+ * All scratch is one fixed device array of DHARA_NOALLOC_MAX_COLUMNS columns
+ * that every GPU loading the library keeps until exit; larger domains return
+ * DHARA_ERR_UNSUPPORTED.  Calls share that array: calls whose GPU work
+ * overlaps race, so order them on one stream.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress); make it before any
+ * stream capture.  Nothing is allocated, nothing is synchronised. */
+#define DHARA_NOALLOC_MAX_COLUMNS 16384
+int dhara_overland_step_noalloc(const dhara_params *p, double *waterdepth, const double *ztopo,
+                                const double *mann, double *waterelev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
