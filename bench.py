@@ -141,13 +141,23 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """Max of a per-rank value over all ranks (device tensor under NCCL, host
+    tensor under gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_throughput(cells_per_rank, steps, ms, world):
+    """Whole-job cell-steps/s of `world` independent replicas: all ranks'
+    cells x steps over the slowest rank's time."""
+    ms_max = max_over_ranks(ms, world)
+    return world * cells_per_rank * steps / (ms_max / 1e3), ms_max
 
 
 # ------------------------------------------------------------------ ours
@@ -205,8 +215,7 @@ def run_ours(args, world, rank, local):
     kbytes, kiters = s.krylov_traffic()
     timing = {k: s.kernel_timing(k) for k in db.KERNELS}
     s.close()
-    ms_max = max_over_ranks(ms, world)
-    value = world * N * args.steps / (ms_max / 1e3)
+    value, ms_max = replica_throughput(N, args.steps, ms, world)
 
     # FP64 solver on the same workload (bounded number of steps)
     fp64_value = None

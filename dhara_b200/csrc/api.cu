@@ -551,8 +551,11 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     return DHARA_OK;
 }
 
+void dhara_internal_forget(dhara_handle *h);  // dropin.cu
+
 int dhara_destroy(dhara_handle *h) {
     if (!h) return DHARA_OK;
+    dhara_internal_forget(h);
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
@@ -652,6 +655,57 @@ int dhara_download(dhara_handle *h, int domain, int field, double *dst, int64_t 
     } else {
         CK(cudaMemcpyAsync(dst, f.ptr, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     }
+    CK(cudaStreamSynchronize(h->stream));
+    return DHARA_OK;
+}
+
+int dhara_upload_device(dhara_handle *h, int domain, int field, const double *dsrc, int64_t count) {
+    if (!h || !dsrc) return fail(DHARA_ERR_INVALID, "NULL handle or source");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    FieldLoc f;
+    int rc = locate(h, domain, field, &f);
+    if (rc) return rc;
+    if (f.is_int || f.computed) return fail(DHARA_ERR_INVALID, "field %d cannot be uploaded from the device", field);
+    if (count != f.count) return fail(DHARA_ERR_INVALID, "field %d expects %lld values, got %lld", field,
+                                      (long long)f.count, (long long)count);
+    if (!f.ptr) return DHARA_OK;
+    const DomainDesc &D = h->hdom[domain];
+    if (f.is3d)
+        CK(cudaMemcpy2DAsync(f.ptr, (size_t)D.nxp * sizeof(double), dsrc, (size_t)D.nx * sizeof(double),
+                             (size_t)D.nx * sizeof(double), (size_t)D.ny * D.nz, cudaMemcpyDeviceToDevice,
+                             h->stream));
+    else
+        CK(cudaMemcpyAsync(f.ptr, dsrc, count * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (field == DHARA_F_PSI) h->uploaded[domain] |= UP_PSI;
+    if (field == DHARA_F_THETA) h->uploaded[domain] |= UP_THETA;
+    if (field == DHARA_F_KSAT) h->uploaded[domain] |= UP_KSAT;
+    if (field == DHARA_F_ZTOPO) h->uploaded[domain] |= UP_ZTOPO;
+    return DHARA_OK;
+}
+
+int dhara_download_device(dhara_handle *h, int domain, int field, double *ddst, int64_t count) {
+    if (!h || !ddst) return fail(DHARA_ERR_INVALID, "NULL handle or destination");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    FieldLoc f;
+    int rc = locate(h, domain, field, &f);
+    if (rc) return rc;
+    if (f.is_int) return fail(DHARA_ERR_INVALID, "field %d is an int32 field", field);
+    if (count != f.count) return fail(DHARA_ERR_INVALID, "field %d holds %lld values, asked %lld", field,
+                                      (long long)f.count, (long long)count);
+    const DomainDesc &D = h->hdom[domain];
+    if (f.computed) {
+        if (!h->scratch && dalloc(h, &h->scratch, (size_t)h->Ntot)) return DHARA_ERR_NOMEM;
+        CK(launch_eval_fields(h->P, f.which, h->scratch, h->stream));
+        f.ptr = h->scratch + D.off3;
+    }
+    if (!f.ptr) return fail(DHARA_ERR_INVALID, "field %d is not stored on the GPU path", field);
+    if (f.is3d)
+        CK(cudaMemcpy2DAsync(ddst, (size_t)D.nx * sizeof(double), f.ptr, (size_t)D.nxp * sizeof(double),
+                             (size_t)D.nx * sizeof(double), (size_t)D.ny * D.nz, cudaMemcpyDeviceToDevice,
+                             h->stream));
+    else
+        CK(cudaMemcpyAsync(ddst, f.ptr, count * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return DHARA_OK;
 }

@@ -197,6 +197,10 @@ int dhara_abi_version(void);
 int dhara_upload(dhara_handle *h, int domain, int field, const double *src, int64_t count);
 int dhara_upload_int(dhara_handle *h, int domain, int field, const int32_t *src, int64_t count);
 int dhara_download(dhara_handle *h, int domain, int field, double *dst, int64_t count);
+/* The same with device pointers (caller-owned device arrays, reference
+ * layout); ordered on the handle's stream and complete on return. */
+int dhara_upload_device(dhara_handle *h, int domain, int field, const double *dsrc, int64_t count);
+int dhara_download_device(dhara_handle *h, int domain, int field, double *ddst, int64_t count);
 /* Root density table rda[proc*nz + k] (src/subsurface.cu:115). */
 int dhara_set_roots(dhara_handle *h, int domain, const double *rda, int nproc);
 /* Optional per-step rain for graph-replayed runs: mm per step, uniform over

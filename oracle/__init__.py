@@ -187,3 +187,102 @@ def run(domain, nsteps=None, solver3d=SOLVER_BICGSTAB, solver2d=SOLVER_CG, recor
     diag = o.diagnostics()
     o.close()
     return state, diag, rec
+
+
+# ---------------------------------------------------------------------------
+# Per-kernel records (oracle/kernel_io.h) and the reference's own kernels
+# compiled from its sources (oracle/_ref/libdhara_refkernels.so, built by
+# `make -C oracle ref` where the reference tree is available).
+
+_dp_t = ct.POINTER(ct.c_double)
+_ip_t = ct.POINTER(ct.c_int)
+
+
+class AsmIO(ct.Structure):
+    _fields_ = [("nx", ct.c_int), ("ny", ct.c_int), ("nz", ct.c_int), ("nproc", ct.c_int)] + [
+        (n, _dp_t) for n in ("psinp1m", "psin", "thetanp1m", "thetan", "knp1m", "cnp1m")] + [
+        (n, _ip_t) for n in ("wbc", "ebc", "sbc", "nbc", "tbc", "bbc")] + [
+        (n, _dp_t) for n in ("psi_w", "psi_e", "psi_s", "psi_n", "psi_t", "psi_b",
+                             "qw", "qe", "qs", "qn", "qt", "qb", "tr")] + [
+        ("procmap", _ip_t), ("root", _dp_t), ("a3d", _dp_t), ("rhs", _dp_t)]
+
+
+class FluxIO(ct.Structure):
+    _fields_ = [("nx", ct.c_int), ("ny", ct.c_int), ("nz", ct.c_int), ("nproc", ct.c_int)] + [
+        (n, _dp_t) for n in ("knp1m", "psinp1mp1", "psin", "thetanp1mp1", "thetan", "E_soil", "TR", "qss",
+                             "bcqw", "bcqe", "bcqs", "bcqn", "bcqt", "bcqb")] + [
+        (n, _ip_t) for n in ("wbc", "ebc", "sbc", "nbc", "tbc", "bbc", "procmap")] + [
+        ("root", _dp_t)] + [
+        (n, _dp_t) for n in ("quflux", "qdflux", "qwflux", "qeflux", "qsflux", "qnflux",
+                             "dtheta", "transp", "evapo", "ssflux")]
+
+
+class TopIO(ct.Structure):
+    _fields_ = [("nx", ct.c_int), ("ny", ct.c_int)] + [
+        (n, _dp_t) for n in ("ph_in", "psinp1m", "knp1m", "ppt", "et", "ksat", "thetan", "psinp1mp1",
+                             "psi_top", "hpoten", "qcapa", "topqflux", "qss", "ph_out")] + [
+        ("topbc", _ip_t)]
+
+
+class OlfIO(ct.Structure):
+    _fields_ = [("nx", ct.c_int), ("ny", ct.c_int)] + [
+        (n, _dp_t) for n in ("waterdepth", "ztopo", "mann", "waterelev", "kw", "ke", "ks", "kn", "a2d",
+                             "rhs2d", "waterdepth_out")]
+
+
+def fill(record, arrays):
+    """Points the record's pointer fields at the numpy arrays (kept alive by
+    the caller) and sets the integer fields."""
+    for name, typ in record._fields_:
+        if name in arrays:
+            v = arrays[name]
+            if typ is ct.c_int:
+                setattr(record, name, int(v))
+            elif typ is _ip_t:
+                setattr(record, name, v.ctypes.data_as(_ip_t))
+            else:
+                setattr(record, name, v.ctypes.data_as(_dp_t))
+    return record
+
+
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libdhara_refkernels.so")
+_ref = None
+
+
+def ref_lib():
+    """The reference's own kernels (None when they were not built)."""
+    global _ref
+    if _ref is None and os.path.exists(REF_LIB_PATH):
+        R = ct.CDLL(REF_LIB_PATH)
+        P = ct.POINTER
+        R.ref_k_van_genuchten.argtypes = [P(_abi.Params), ct.c_longlong, _dp_t, _dp_t, _dp_t, _dp_t, _dp_t]
+        R.ref_k_vg_inverse.argtypes = [P(_abi.Params), ct.c_longlong, _dp_t, _dp_t]
+        R.ref_k_top.argtypes = [P(_abi.Params), P(TopIO)]
+        R.ref_k_infiltration.argtypes = [P(_abi.Params), P(TopIO)]
+        R.ref_k_assemble.argtypes = [P(_abi.Params), P(AsmIO)]
+        R.ref_k_water_flux.argtypes = [P(_abi.Params), P(FluxIO)]
+        R.ref_k_overland_setup.argtypes = [P(_abi.Params), P(OlfIO)]
+        R.ref_k_water_depth.argtypes = [P(_abi.Params), P(OlfIO)]
+        _ref = R
+    return _ref
+
+
+def _k(name, *argtypes):
+    fn = getattr(lib(), name)
+    fn.argtypes = list(argtypes)
+    fn.restype = None
+    return fn
+
+
+def k_functions():
+    """The oracle's stateless per-kernel restatements."""
+    P = ct.POINTER
+    return dict(
+        assemble=_k("oracle_k_assemble", P(_abi.Params), P(AsmIO)),
+        estimate_fluxes=_k("oracle_k_estimate_fluxes", P(_abi.Params), P(TopIO)),
+        identify_top=_k("oracle_k_identify_top", P(_abi.Params), P(TopIO)),
+        infiltration=_k("oracle_k_infiltration", P(_abi.Params), P(TopIO)),
+        water_flux=_k("oracle_k_water_flux", P(_abi.Params), P(FluxIO)),
+        overland_setup=_k("oracle_k_overland_setup", P(_abi.Params), P(OlfIO)),
+        water_depth=_k("oracle_k_water_depth", P(_abi.Params), P(OlfIO)),
+    )

@@ -12,6 +12,7 @@
 // values it is given.  Loops are OpenMP-parallel so the same code serves as
 // the multi-core CPU baseline.
 #include "dhara_oracle.h"
+#include "kernel_io.h"
 
 #include <cmath>
 #include <cstring>
@@ -398,7 +399,7 @@ extern "C" int oracle_prepare(dhara_oracle *o) {
 // ------------------------------------------------------------- subsurface
 // HydraulicConductivityAtInterface (src/subsurface.cu:26-79): arithmetic mean,
 // zero on domain faces.
-static inline void face_k(const vec &K, long g, int i, int j, int k, int nx, int ny, int nz,
+static inline void face_k(const double *K, long g, int i, int j, int k, int nx, int ny, int nz,
                           double *ke, double *kw, double *kn, double *ks, double *ku, double *kd) {
     const long sxy = (long)nx * ny;
     *kd = (k == 0) ? 0 : 0.5 * (K[g] + K[g - sxy]);
@@ -412,13 +413,13 @@ static inline void face_k(const vec &K, long g, int i, int j, int k, int nx, int
 // SetUpLinearSystemsSubsurface (src/subsurface.cu:381-429) with
 // SetUpBlockMatrixSubsurface (83-102), SetUpRightHandSideSubsurface (106-122)
 // and SetUpBoundaryConditionsSubsurface (126-353) inlined in reference order.
-static void assemble(dhara_oracle *o) {
-    const dhara_params &P = o->p;
-    const int nx = o->nx, ny = o->ny, nz = o->nz;
-    const long sxy = o->nxy, N = o->N;
+extern "C" void oracle_k_assemble(const dhara_params *pp, const oracle_asm_io *io) {
+    const dhara_params &P = *pp;
+    const int nx = io->nx, ny = io->ny, nz = io->nz;
+    const long sxy = (long)nx * ny, N = sxy * nz;
     const double dx = P.dx, dy = P.dy, dz = P.dz, dt = P.dt;
     const double Ss = P.Ss, poros = P.porosity, sec = P.sec_p_mm2dt_p_m;
-    double *a3d = o->a3d.data(), *rhs = o->rhs3d.data();
+    double *a3d = io->a3d, *rhs = io->rhs;
 #pragma omp parallel for schedule(static)
     for (long tid = 0; tid < N; ++tid) {
         const int k = (int)(tid / sxy);
@@ -427,70 +428,86 @@ static void assemble(dhara_oracle *o) {
         const double dx2inv = -1.0 / (dx * dx), dy2inv = -1.0 / (dy * dy), dz2inv = -1.0 / (dz * dz);
         const long g = tid;
         double ke, kw, kn, ks, ku, kd;
-        face_k(o->knp1m, g, i, j, k, nx, ny, nz, &ke, &kw, &kn, &ks, &ku, &kd);
+        face_k(io->knp1m, g, i, j, k, nx, ny, nz, &ke, &kw, &kn, &ks, &ku, &kd);
         // block matrix
         a3d[0 * N + tid] = dz2inv * kd;
         a3d[1 * N + tid] = dy2inv * ks;
         a3d[2 * N + tid] = dx2inv * kw;
-        a3d[3 * N + tid] = Ss / dt * o->thetanp1m[g] / poros + o->cnp1m[g] / dt - (ke + kw) * dx2inv -
+        a3d[3 * N + tid] = Ss / dt * io->thetanp1m[g] / poros + io->cnp1m[g] / dt - (ke + kw) * dx2inv -
                            (kn + ks) * dy2inv - (ku + kd) * dz2inv;
         a3d[4 * N + tid] = dx2inv * ke;
         a3d[5 * N + tid] = dy2inv * kn;
         a3d[6 * N + tid] = dz2inv * ku;
         // right-hand side
         const long id2d = (long)j * nx + i;
-        const int proc = o->procmap[id2d];
+        const int proc = io->procmap[id2d];
         double trodz;
-        if (o->tr[id2d] > 0)
-            trodz = -o->tr[id2d] * o->rda[(long)proc * nz + k] * sec / dz;
+        if (io->tr[id2d] > 0)
+            trodz = -io->tr[id2d] * io->root[(long)proc * nz + k] * sec / dz;
         else
             trodz = 0;
-        rhs[tid] = Ss / dt * o->thetanp1m[g] / poros * o->psin[g] + o->cnp1m[g] / dt * o->psinp1m[g] -
-                   (ku - kd) / dz + (o->thetan[g] - o->thetanp1m[g]) / dt + trodz / dt;
+        rhs[tid] = Ss / dt * io->thetanp1m[g] / poros * io->psin[g] + io->cnp1m[g] / dt * io->psinp1m[g] -
+                   (ku - kd) / dz + (io->thetan[g] - io->thetanp1m[g]) / dt + trodz / dt;
         // boundary conditions
         const long bi = (long)k * ny + j, bj = (long)k * nx + i, bk = (long)j * nx + i;
         auto identity_row = [&](double v) {
             for (int r = 0; r < 7; ++r) a3d[r * N + tid] = (r == 3) ? 1.0 : 0.0;
             rhs[tid] = v;
         };
-        if (o->bct[bk] == 0) {
-            if (k == 1) { a3d[0 * N + tid] = 0.0; rhs[tid] -= dz2inv * kd * o->bcpsit[bk]; }
-            if (k == 0) identity_row(o->bcpsit[bk]);
+        if (io->tbc[bk] == 0) {
+            if (k == 1) { a3d[0 * N + tid] = 0.0; rhs[tid] -= dz2inv * kd * io->psi_t[bk]; }
+            if (k == 0) identity_row(io->psi_t[bk]);
         } else if (k == 0) {
-            rhs[tid] += (-o->bcqt[bk] * dz) * dz2inv;
+            rhs[tid] += (-io->qt[bk] * dz) * dz2inv;
         }
-        if (o->bcb[bk] == 0) {
-            if (k == nz - 2) { a3d[6 * N + tid] = 0.0; rhs[tid] -= dz2inv * ku * o->bcpsib[bk]; }
-            if (k == nz - 1) identity_row(o->bcpsib[bk]);
+        if (io->bbc[bk] == 0) {
+            if (k == nz - 2) { a3d[6 * N + tid] = 0.0; rhs[tid] -= dz2inv * ku * io->psi_b[bk]; }
+            if (k == nz - 1) identity_row(io->psi_b[bk]);
         } else if (k == nz - 1) {
-            o->bcqb[bk] = o->knp1m[tid];
-            rhs[tid] += (o->bcqb[bk] * dz) * dz2inv;
+            io->qb[bk] = io->knp1m[tid];
+            rhs[tid] += (io->qb[bk] * dz) * dz2inv;
         }
-        if (o->bcs[bj] == 0) {
-            if (j == 1) { a3d[1 * N + tid] = 0.0; rhs[tid] -= dy2inv * kn * o->bcpsis[bj]; }
-            if (j == 0) identity_row(o->bcpsis[bj]);
+        if (io->sbc[bj] == 0) {
+            if (j == 1) { a3d[1 * N + tid] = 0.0; rhs[tid] -= dy2inv * kn * io->psi_s[bj]; }
+            if (j == 0) identity_row(io->psi_s[bj]);
         } else if (j == 0) {
-            rhs[tid] += (-o->bcqs[bj] * dy) * dy2inv;
+            rhs[tid] += (-io->qs[bj] * dy) * dy2inv;
         }
-        if (o->bcn[bj] == 0) {
-            if (j == ny - 2) { a3d[5 * N + tid] = 0.0; rhs[tid] -= dy2inv * ks * o->bcpsin[bj]; }
-            if (j == ny - 1) identity_row(o->bcpsin[bj]);
+        if (io->nbc[bj] == 0) {
+            if (j == ny - 2) { a3d[5 * N + tid] = 0.0; rhs[tid] -= dy2inv * ks * io->psi_n[bj]; }
+            if (j == ny - 1) identity_row(io->psi_n[bj]);
         } else if (j == ny - 1) {
-            rhs[tid] += (o->bcqn[bj] * dy) * dy2inv;
+            rhs[tid] += (io->qn[bj] * dy) * dy2inv;
         }
-        if (o->bcw[bi] == 0) {
-            if (i == 1) { a3d[2 * N + tid] = 0.0; rhs[tid] -= dx2inv * ke * o->bcpsiw[bi]; }
-            if (i == 0) identity_row(o->bcpsiw[bi]);
+        if (io->wbc[bi] == 0) {
+            if (i == 1) { a3d[2 * N + tid] = 0.0; rhs[tid] -= dx2inv * ke * io->psi_w[bi]; }
+            if (i == 0) identity_row(io->psi_w[bi]);
         } else if (i == 0) {
-            rhs[tid] += (-o->bcqw[bi] * dx) * dx2inv;
+            rhs[tid] += (-io->qw[bi] * dx) * dx2inv;
         }
-        if (o->bce[bi] == 0) {
-            if (i == nx - 2) { a3d[4 * N + tid] = 0.0; rhs[tid] -= dx2inv * kw * o->bcpsie[bi]; }
-            if (i == nx - 1) identity_row(o->bcpsie[bi]);
+        if (io->ebc[bi] == 0) {
+            if (i == nx - 2) { a3d[4 * N + tid] = 0.0; rhs[tid] -= dx2inv * kw * io->psi_e[bi]; }
+            if (i == nx - 1) identity_row(io->psi_e[bi]);
         } else if (i == nx - 1) {
-            rhs[tid] += (o->bcqe[bi] * dx) * dx2inv;
+            rhs[tid] += (io->qe[bi] * dx) * dx2inv;
         }
     }
+}
+
+static void assemble(dhara_oracle *o) {
+    oracle_asm_io io;
+    io.nx = o->nx; io.ny = o->ny; io.nz = o->nz; io.nproc = o->nproc;
+    io.psinp1m = o->psinp1m.data(); io.psin = o->psin.data(); io.thetanp1m = o->thetanp1m.data();
+    io.thetan = o->thetan.data(); io.knp1m = o->knp1m.data(); io.cnp1m = o->cnp1m.data();
+    io.wbc = o->bcw.data(); io.ebc = o->bce.data(); io.sbc = o->bcs.data(); io.nbc = o->bcn.data();
+    io.tbc = o->bct.data(); io.bbc = o->bcb.data();
+    io.psi_w = o->bcpsiw.data(); io.psi_e = o->bcpsie.data(); io.psi_s = o->bcpsis.data();
+    io.psi_n = o->bcpsin.data(); io.psi_t = o->bcpsit.data(); io.psi_b = o->bcpsib.data();
+    io.qw = o->bcqw.data(); io.qe = o->bcqe.data(); io.qs = o->bcqs.data(); io.qn = o->bcqn.data();
+    io.qt = o->bcqt.data(); io.qb = o->bcqb.data();
+    io.tr = o->tr.data(); io.procmap = o->procmap.data(); io.root = o->rda.data();
+    io.a3d = o->a3d.data(); io.rhs = o->rhs3d.data();
+    oracle_k_assemble(&o->p, &io);
 }
 
 extern "C" int oracle_assemble(dhara_oracle *o, double *a3d, double *rhs) {
@@ -500,71 +517,130 @@ extern "C" int oracle_assemble(dhara_oracle *o, double *a3d, double *rhs) {
     return DHARA_OK;
 }
 
-// WaterFluxEstimate (src/subsurface.cu:494-629) followed by the nine
-// reductions and the water balance of src/subsurface.cu:809-826.
-static double water_balance(dhara_oracle *o) {
-    const dhara_params &P = o->p;
-    const int N = o->nx, M = o->ny, Pz = o->nz;
-    const long sxy = o->nxy, NN = o->N;
-    const double dx = P.dx, dy = P.dy, dz = P.dz, dt = P.dt;
-    const vec &K = o->knp1m, &psi = o->psinp1mp1;
-#pragma omp parallel for schedule(static)
-    for (long tid = 0; tid < NN; ++tid) {
-        o->qdflux[tid] = o->quflux[tid] = o->qwflux[tid] = o->qeflux[tid] = o->qsflux[tid] =
-            o->qnflux[tid] = 0;
+// EstimateFluxes (src/global.cu:172-191) on the top layer.
+extern "C" void oracle_k_estimate_fluxes(const dhara_params *p, const oracle_top_io *io) {
+    const long C = (long)io->nx * io->ny;
+    const double dt = p->dt, dz = p->dz;
+    for (long tid = 0; tid < C; ++tid) {
+        io->hpoten[tid] = io->ph_in[tid] + io->ppt[tid] / 1000 - io->et[tid] * p->sec_p_mm2dt_p_m * dt;
+        io->qcapa[tid] = -io->knp1m[tid] * ((io->psinp1m[tid] - io->hpoten[tid] - 0.5 * dz) / (0.5 * dz));
+        if (io->ph_in[tid] / dt > io->ksat[tid]) io->qcapa[tid] = maxcomp(io->qcapa[tid], io->ksat[tid]);
     }
+}
+
+// IdentifyTopBoundary (src/global.cu:206-257).
+extern "C" void oracle_k_identify_top(const dhara_params *p, const oracle_top_io *io) {
+    const long C = (long)io->nx * io->ny;
+    const double dt = p->dt, dz = p->dz;
+    for (long tid = 0; tid < C; ++tid) {
+        io->topbc[tid] = 1;
+        if (io->hpoten[tid] > 0.0) {
+            if (io->hpoten[tid] / dt > io->qcapa[tid])
+                io->topqflux[tid] = io->qcapa[tid];
+            else
+                io->topqflux[tid] = io->hpoten[tid] / dt;
+            io->topqflux[tid] = mincomp(io->topqflux[tid], (p->theta_s - io->thetan[tid]) * dz / dt);
+            io->topqflux[tid] = mincomp(io->topqflux[tid], io->ksat[tid]);
+        } else {
+            io->topqflux[tid] = io->hpoten[tid] / dt;
+        }
+    }
+}
+
+// SubsurfaceEstimateInfiltrationPonding (src/subsurface.cu:465-491).
+extern "C" void oracle_k_infiltration(const dhara_params *p, const oracle_top_io *io) {
+    const long C = (long)io->nx * io->ny;
+    const double dt = p->dt, dz = p->dz;
+    for (long tid = 0; tid < C; ++tid) {
+        if (io->topbc[tid] == 1) {
+            io->qss[tid] = io->topqflux[tid];
+            io->ph_out[tid] = maxcomp(io->hpoten[tid] - io->qss[tid] * dt, 0.0);
+        } else {
+            io->qss[tid] = -io->knp1m[tid] * (io->psinp1mp1[tid] - io->psi_top[tid] - dz) / dz;
+            io->ph_out[tid] = maxcomp(io->psi_top[tid] - io->qss[tid] * dt, 0.0);
+        }
+    }
+}
+
+// WaterFluxEstimate (src/subsurface.cu:494-629).
+extern "C" void oracle_k_water_flux(const dhara_params *pp, const oracle_flux_io *io) {
+    const dhara_params &P = *pp;
+    const int N = io->nx, M = io->ny, Pz = io->nz;
+    const long sxy = (long)N * M, NN = sxy * Pz;
+    const double dx = P.dx, dy = P.dy, dz = P.dz, dt = P.dt;
+    const double *K = io->knp1m, *psi = io->psinp1mp1;
     // Dirichlet faces make a cell write its neighbour's flux; run serially in
     // that case to keep the reference's last-writer order.
     bool any_dirichlet = false;
-    for (int v : o->bcb) any_dirichlet |= (v == 0);
-    for (int v : o->bcw) any_dirichlet |= (v == 0);
-    for (int v : o->bce) any_dirichlet |= (v == 0);
-    for (int v : o->bcs) any_dirichlet |= (v == 0);
-    for (int v : o->bcn) any_dirichlet |= (v == 0);
+    for (long q = 0; q < sxy; ++q) any_dirichlet |= (io->bbc[q] == 0);
+    for (long q = 0; q < (long)Pz * M; ++q) any_dirichlet |= (io->wbc[q] == 0) | (io->ebc[q] == 0);
+    for (long q = 0; q < (long)Pz * N; ++q) any_dirichlet |= (io->sbc[q] == 0) | (io->nbc[q] == 0);
 #pragma omp parallel for schedule(static) if (!any_dirichlet)
     for (long tid = 0; tid < NN; ++tid) {
         const int k = (int)(tid / sxy);
         const int j = (int)((tid % sxy) / N);
         const int i = (int)((tid % sxy) % N);
         const long g = tid, id2d = (long)j * N + i;
-        const int proc = o->procmap[id2d];
+        const int proc = io->procmap[id2d];
         const long bi = (long)k * M + j, bj = (long)k * N + i, bk = (long)j * N + i;
         double ke, kw, kn, ks, ku, kd;
         face_k(K, g, i, j, k, N, M, Pz, &ke, &kw, &kn, &ks, &ku, &kd);
-        if (k != 0) o->qdflux[g] = kd * ((psi[g - sxy] - psi[g]) / dz + 1);
+        io->qdflux[g] = 0; io->quflux[g] = 0; io->qwflux[g] = 0;
+        io->qeflux[g] = 0; io->qsflux[g] = 0; io->qnflux[g] = 0;
+        if (k != 0) io->qdflux[g] = kd * ((psi[g - sxy] - psi[g]) / dz + 1);
         if (k != Pz - 1) {
-            o->quflux[g] = ku * ((psi[g] - psi[g + sxy]) / dz + 1);
-            if (o->bcb[bk] == 0) o->quflux[g + sxy] = ku * ((psi[g] - psi[g + sxy]) / dz + 1);
+            io->quflux[g] = ku * ((psi[g] - psi[g + sxy]) / dz + 1);
+            if (io->bbc[bk] == 0) io->quflux[g + sxy] = ku * ((psi[g] - psi[g + sxy]) / dz + 1);
         }
         if (i != 0) {
-            o->qwflux[g] = kw * (psi[g - 1] - psi[g]) / dx;
-            if (o->bcw[bi] == 0) o->qwflux[g - 1] = kw * (psi[g - 1] - psi[g]) / dx;
+            io->qwflux[g] = kw * (psi[g - 1] - psi[g]) / dx;
+            if (io->wbc[bi] == 0) io->qwflux[g - 1] = kw * (psi[g - 1] - psi[g]) / dx;
         }
         if (i != N - 1) {
-            o->qeflux[g] = ke * (psi[g] - psi[g + 1]) / dx;
-            if (o->bce[bi] == 0) o->qeflux[g + 1] = ke * (psi[g] - psi[g + 1]) / dx;
+            io->qeflux[g] = ke * (psi[g] - psi[g + 1]) / dx;
+            if (io->ebc[bi] == 0) io->qeflux[g + 1] = ke * (psi[g] - psi[g + 1]) / dx;
         }
         if (j != 0) {
-            o->qsflux[g] = ks * (psi[g - N] - psi[g]) / dy;
-            if (o->bcs[bj] == 0) o->qsflux[g - N] = ks * (psi[g - N] - psi[g]) / dy;
+            io->qsflux[g] = ks * (psi[g - N] - psi[g]) / dy;
+            if (io->sbc[bj] == 0) io->qsflux[g - N] = ks * (psi[g - N] - psi[g]) / dy;
         }
         if (j != M - 1) {
-            o->qnflux[g] = kn * (psi[g] - psi[g + N]) / dy;
-            if (o->bcn[bj] == 0) o->qnflux[g + N] = kn * (psi[g] - psi[g + N]) / dy;
+            io->qnflux[g] = kn * (psi[g] - psi[g + N]) / dy;
+            if (io->nbc[bj] == 0) io->qnflux[g + N] = kn * (psi[g] - psi[g + N]) / dy;
         }
-        if (k == 0) o->qdflux[g] = o->bcqt[bk];
-        if (k == Pz - 1 && o->bcb[bk] != 0) o->quflux[g] = o->bcqb[bk];
-        if (i == N - 1 && o->bce[bi] != 0) o->qeflux[g] = o->bcqe[bi];
-        if (i == 0 && o->bcw[bi] != 0) o->qwflux[g] = o->bcqw[bi];
-        if (j == M - 1 && o->bcn[bj] != 0) o->qnflux[g] = o->bcqn[bj];
-        if (j == 0 && o->bcs[bj] != 0) o->qsflux[g] = o->bcqs[bj];
-        o->dtheta[g] = o->thetanp1mp1[g] - o->thetan[g];
-        if (o->tr[id2d] > 0)
-            o->transp[g] = -o->tr[id2d] * P.sec_p_mm2dt_p_m * o->rda[(long)proc * Pz + k];
+        if (k == 0) io->qdflux[g] = io->bcqt[bk];
+        if (k == Pz - 1 && io->bbc[bk] != 0) io->quflux[g] = io->bcqb[bk];
+        if (i == N - 1 && io->ebc[bi] != 0) io->qeflux[g] = io->bcqe[bi];
+        if (i == 0 && io->wbc[bi] != 0) io->qwflux[g] = io->bcqw[bi];
+        if (j == M - 1 && io->nbc[bj] != 0) io->qnflux[g] = io->bcqn[bj];
+        if (j == 0 && io->sbc[bj] != 0) io->qsflux[g] = io->bcqs[bj];
+        io->dtheta[g] = io->thetanp1mp1[g] - io->thetan[g];
+        if (io->TR[id2d] > 0)
+            io->transp[g] = -io->TR[id2d] * P.sec_p_mm2dt_p_m * io->root[(long)proc * Pz + k];
         else
-            o->transp[g] = 0;
-        o->ssflux[g] = (psi[g] - o->psin[g]) * (P.Ss / dt * o->thetanp1mp1[g] / P.porosity) * dz;
+            io->transp[g] = 0;
+        io->ssflux[g] = (psi[g] - io->psin[g]) * (P.Ss / dt * io->thetanp1mp1[g] / P.porosity) * dz;
     }
+}
+
+// The nine reductions and the water balance of src/subsurface.cu:809-826.
+static double water_balance(dhara_oracle *o) {
+    oracle_flux_io io;
+    io.nx = o->nx; io.ny = o->ny; io.nz = o->nz; io.nproc = o->nproc;
+    io.knp1m = o->knp1m.data(); io.psinp1mp1 = o->psinp1mp1.data(); io.psin = o->psin.data();
+    io.thetanp1mp1 = o->thetanp1mp1.data(); io.thetan = o->thetan.data();
+    io.E_soil = o->esoil.data(); io.TR = o->tr.data(); io.qss = o->qss.data();
+    io.bcqw = o->bcqw.data(); io.bcqe = o->bcqe.data(); io.bcqs = o->bcqs.data(); io.bcqn = o->bcqn.data();
+    io.bcqt = o->bcqt.data(); io.bcqb = o->bcqb.data();
+    io.wbc = o->bcw.data(); io.ebc = o->bce.data(); io.sbc = o->bcs.data(); io.nbc = o->bcn.data();
+    io.tbc = o->bct.data(); io.bbc = o->bcb.data();
+    io.procmap = o->procmap.data(); io.root = o->rda.data();
+    io.quflux = o->quflux.data(); io.qdflux = o->qdflux.data(); io.qwflux = o->qwflux.data();
+    io.qeflux = o->qeflux.data(); io.qsflux = o->qsflux.data(); io.qnflux = o->qnflux.data();
+    io.dtheta = o->dtheta.data(); io.transp = o->transp.data(); io.evapo = nullptr; io.ssflux = o->ssflux.data();
+    oracle_k_water_flux(&o->p, &io);
+    const long NN = o->N;
+    const double dz = o->p.dz, dt = o->p.dt;
     double s_qu = 0, s_qd = 0, s_qw = 0, s_qe = 0, s_qs = 0, s_qn = 0, s_ss = 0, s_tr = 0, s_dt = 0;
 #pragma omp parallel for schedule(static) reduction(+ : s_qu, s_qd, s_qw, s_qe, s_qs, s_qn, s_ss, s_tr, s_dt)
     for (long g = 0; g < NN; ++g) {
@@ -573,6 +649,17 @@ static double water_balance(dhara_oracle *o) {
         s_ss += o->ssflux[g]; s_tr += o->transp[g]; s_dt += o->dtheta[g];
     }
     return s_dt * dz + ((s_qe - s_qw) + (s_qn - s_qs) + (s_qu - s_qd)) * dt - s_tr + s_ss * dt;
+}
+
+static oracle_top_io top_io(dhara_oracle *o) {
+    oracle_top_io io;
+    io.nx = o->nx; io.ny = o->ny;
+    io.ph_in = o->ph.data(); io.psinp1m = o->psinp1m.data(); io.knp1m = o->knp1m.data();
+    io.ppt = o->ppt.data(); io.et = o->esoil.data(); io.ksat = o->ksat.data(); io.thetan = o->thetan.data();
+    io.psinp1mp1 = o->psinp1mp1.data(); io.psi_top = o->bcpsit.data();
+    io.hpoten = o->hpoten.data(); io.qcapa = o->qcapa.data(); io.topqflux = o->bcqt.data();
+    io.qss = o->qss.data(); io.ph_out = o->ph.data(); io.topbc = o->bct.data();
+    return io;
 }
 
 // SubsurfaceFlowModel (src/subsurface.cu:686-847).  rain_mm, when given,
@@ -586,12 +673,8 @@ extern "C" int oracle_subsurface_step(dhara_oracle *o, const double *rain_mm) {
         for (long c = 0; c < C; ++c) o->ppt[c] = *rain_mm;
     // psinp1m <- psin (:704)
     o->psinp1m = o->psin;
-    // EstimateFluxes (src/global.cu:172-191) on the top layer
-    for (long tid = 0; tid < C; ++tid) {
-        o->hpoten[tid] = o->ph[tid] + o->ppt[tid] / 1000 - o->esoil[tid] * P.sec_p_mm2dt_p_m * dt;
-        o->qcapa[tid] = -o->knp1m[tid] * ((o->psinp1m[tid] - o->hpoten[tid] - 0.5 * dz) / (0.5 * dz));
-        if (o->ph[tid] / dt > o->ksat[tid]) o->qcapa[tid] = maxcomp(o->qcapa[tid], o->ksat[tid]);
-    }
+    const oracle_top_io tio = top_io(o);
+    oracle_k_estimate_fluxes(&P, &tio);
     const long lnoff[7] = {-C, -(long)o->nx, -1, 0, 1, (long)o->nx, C};
     int runflag = 0, niter = 0;
     const int maxiter = P.picard_maxiter;
@@ -599,20 +682,7 @@ extern "C" int oracle_subsurface_step(dhara_oracle *o, const double *rain_mm) {
     long kry_iters = 0;
     while (runflag == 0 && niter < maxiter) {
         vg_field(o, o->psinp1m, o->cnp1m, o->thetanp1m, o->knp1m);
-        // IdentifyTopBoundary (src/global.cu:206-257)
-        for (long tid = 0; tid < C; ++tid) {
-            o->bct[tid] = 1;
-            if (o->hpoten[tid] > 0.0) {
-                if (o->hpoten[tid] / dt > o->qcapa[tid])
-                    o->bcqt[tid] = o->qcapa[tid];
-                else
-                    o->bcqt[tid] = o->hpoten[tid] / dt;
-                o->bcqt[tid] = mincomp(o->bcqt[tid], (P.theta_s - o->thetan[tid]) * dz / dt);
-                o->bcqt[tid] = mincomp(o->bcqt[tid], o->ksat[tid]);
-            } else {
-                o->bcqt[tid] = o->hpoten[tid] / dt;
-            }
-        }
+        oracle_k_identify_top(&P, &tio);
         assemble(o);
         if (P.theta_update == DHARA_THETA_CONSERVATIVE) {
             o->cm_saved = o->cnp1m;
@@ -650,16 +720,7 @@ extern "C" int oracle_subsurface_step(dhara_oracle *o, const double *rain_mm) {
                 o->psinp1m[t] = P.am * o->psinp1m[t] + (1 - P.am) * o->psinp1mp1[t];
         }
     }
-    // SubsurfaceEstimateInfiltrationPonding (src/subsurface.cu:465-491)
-    for (long tid = 0; tid < C; ++tid) {
-        if (o->bct[tid] == 1) {
-            o->qss[tid] = o->bcqt[tid];
-            o->ph[tid] = maxcomp(o->hpoten[tid] - o->qss[tid] * dt, 0.0);
-        } else {
-            o->qss[tid] = -o->knp1m[tid] * (o->psinp1mp1[tid] - o->bcpsit[tid] - dz) / dz;
-            o->ph[tid] = maxcomp(o->bcpsit[tid] - o->qss[tid] * dt, 0.0);
-        }
-    }
+    oracle_k_infiltration(&P, &tio);
     const double mb = water_balance(o);
     o->diag.mb_subsurface_last = mb;
     o->diag.mb_subsurface_cum += mb;
@@ -757,8 +818,46 @@ extern "C" void oracle_update_k_overland(const dhara_params *p, const double *Hs
     }
 }
 
-// OverlandFlowModel (src/overland.cu:387-419) with WaterElevationOverland
-// (33-45), SetUpLinearSystemsOverland (65-189) and WaterDepthOverland (371-383).
+// WaterElevationOverland (src/overland.cu:33-45), UpdateKOverland (193-368) and
+// SetUpLinearSystemsOverland (65-189) with ppt = et = infil = 0 as called at
+// src/overland.cu:403-406.
+extern "C" void oracle_k_overland_setup(const dhara_params *p, const oracle_olf_io *io) {
+    const int nx = io->nx, ny = io->ny;
+    const long C = (long)nx * ny;
+    const double dt = p->dt, dx = p->dx, dy = p->dy;
+    for (long c = 0; c < C; ++c) io->waterelev[c] = io->waterdepth[c] + io->ztopo[c];
+    oracle_update_k_overland(p, io->waterelev, io->waterdepth, io->mann, io->kw, io->ke, io->ks, io->kn);
+    double *a2d = io->a2d;
+    for (long tid = 0; tid < C; ++tid) {
+        const int i = (int)(tid % nx), j = (int)(tid / nx);
+        const double dtodx2 = -dt / (dx * dx), dtody2 = -dt / (dy * dy);
+        const double waterdepth = 0.0;
+        io->rhs2d[tid] = io->waterelev[tid] + 0. + 0. + 0.;
+        if (i == nx - 1) io->ke[tid] = 0;
+        if (i == 0) io->kw[tid] = 0;
+        if (j == ny - 1) io->kn[tid] = 0;
+        if (j == 0) io->ks[tid] = 0;
+        a2d[0 * C + tid] = dtody2 * io->ks[tid];
+        a2d[1 * C + tid] = dtodx2 * io->kw[tid];
+        a2d[2 * C + tid] = 1.0 - dtodx2 * (io->ke[tid] + io->kw[tid]) - dtody2 * (io->kn[tid] + io->ks[tid]);
+        a2d[3 * C + tid] = dtodx2 * io->ke[tid];
+        a2d[4 * C + tid] = dtody2 * io->kn[tid];
+        if (j == 0 || j == ny - 1 || i == 0 || i == nx - 1) {
+            for (int k = 0; k < 5; ++k) a2d[k * C + tid] = 0.0;
+            a2d[2 * C + tid] = 1.0;
+            io->rhs2d[tid] = io->waterelev[tid] + waterdepth;
+        }
+    }
+}
+
+// WaterDepthOverland (src/overland.cu:371-383).
+extern "C" void oracle_k_water_depth(const dhara_params *p, const oracle_olf_io *io) {
+    const long C = (long)io->nx * io->ny;
+    (void)p;
+    for (long c = 0; c < C; ++c) io->waterdepth_out[c] = maxcomp(io->waterelev[c] - io->ztopo[c], 0.0);
+}
+
+// OverlandFlowModel (src/overland.cu:387-419).
 extern "C" int oracle_overland_step(dhara_oracle *o) {
     if (!o->prepared) return DHARA_ERR_STATE;
     const dhara_params &P = o->p;
@@ -766,33 +865,13 @@ extern "C" int oracle_overland_step(dhara_oracle *o) {
     const long C = o->nxy;
     const double dt = P.dt, dx = P.dx, dy = P.dy;
     vec &H = o->waterelev, &h = o->waterdepth;
-    vec h_before = h;
-    for (long c = 0; c < C; ++c) H[c] = h[c] + o->ztopo[c];
-    oracle_update_k_overland(&P, H.data(), h.data(), o->mann.data(), o->kw2.data(), o->ke2.data(),
-                             o->ks2.data(), o->kn2.data());
-    double *a2d = o->a2d.data();
-    for (long tid = 0; tid < C; ++tid) {
-        const int i = (int)(tid % nx), j = (int)(tid / nx);
-        const double dtodx2 = -dt / (dx * dx), dtody2 = -dt / (dy * dy);
-        const double waterdepth = 0.0;
-        o->rhs2d[tid] = H[tid] + 0. + 0. + 0.;
-        if (i == nx - 1) o->ke2[tid] = 0;
-        if (i == 0) o->kw2[tid] = 0;
-        if (j == ny - 1) o->kn2[tid] = 0;
-        if (j == 0) o->ks2[tid] = 0;
-        a2d[0 * C + tid] = dtody2 * o->ks2[tid];
-        a2d[1 * C + tid] = dtodx2 * o->kw2[tid];
-        a2d[2 * C + tid] = 1.0 - dtodx2 * (o->ke2[tid] + o->kw2[tid]) - dtody2 * (o->kn2[tid] + o->ks2[tid]);
-        a2d[3 * C + tid] = dtodx2 * o->ke2[tid];
-        a2d[4 * C + tid] = dtody2 * o->kn2[tid];
-        if (j == 0 || j == ny - 1 || i == 0 || i == nx - 1) {
-            for (int k = 0; k < 5; ++k) a2d[k * C + tid] = 0.0;
-            a2d[2 * C + tid] = 1.0;
-            o->rhs2d[tid] = H[tid] + waterdepth;
-        }
-    }
+    oracle_olf_io io;
+    io.nx = nx; io.ny = ny;
+    io.waterdepth = h.data(); io.ztopo = o->ztopo.data(); io.mann = o->mann.data();
+    io.waterelev = H.data(); io.kw = o->kw2.data(); io.ke = o->ke2.data(); io.ks = o->ks2.data();
+    io.kn = o->kn2.data(); io.a2d = o->a2d.data(); io.rhs2d = o->rhs2d.data(); io.waterdepth_out = h.data();
+    oracle_k_overland_setup(&P, &io);
     const long off[5] = {-(long)nx, -1, 0, 1, (long)nx};
-    vec Hold = H;
     Monitor mon(o->rhs2d, P.overland_maxiter, P.overland_tol);
     solve(o->solver2d, o->a2d, off, 5, H, o->rhs2d, mon);
     o->diag.overland_iters_total += mon.count;
@@ -810,14 +889,13 @@ extern "C" int oracle_overland_step(dhara_oracle *o) {
     }
     for (long c = 0; c < C; ++c) {
         const double d = H[c] - o->ztopo[c];
-        h[c] = maxcomp(d, 0.0);
         if (d < 0) clip += -d;
-        vol += h[c];
     }
+    oracle_k_water_depth(&P, &io);
+    for (long c = 0; c < C; ++c) vol += h[c];
     o->ph = h;
     o->diag.overland_boundary_out_cum += out;
     o->diag.overland_clip_cum += clip;
     o->diag.ponded_volume = vol;
-    (void)h_before;
     return DHARA_OK;
 }

@@ -20,6 +20,7 @@
 #define DHARA_ORACLE_H
 
 #include "../include/dhara_gpu.h"
+#include "kernel_io.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -67,6 +68,16 @@ int oracle_assemble(dhara_oracle *o, double *a3d, double *rhs);
 void oracle_update_k_overland(const dhara_params *p, const double *H, const double *h,
                               const double *mann, double *kw, double *ke, double *ks,
                               double *kn);
+
+/* Stateless restatements of the reference kernels, one per kernel, on the
+ * records of kernel_io.h.  The oracle's time stepping runs through these. */
+void oracle_k_assemble(const dhara_params *p, const oracle_asm_io *io);
+void oracle_k_estimate_fluxes(const dhara_params *p, const oracle_top_io *io);
+void oracle_k_identify_top(const dhara_params *p, const oracle_top_io *io);
+void oracle_k_infiltration(const dhara_params *p, const oracle_top_io *io);
+void oracle_k_water_flux(const dhara_params *p, const oracle_flux_io *io);
+void oracle_k_overland_setup(const dhara_params *p, const oracle_olf_io *io);
+void oracle_k_water_depth(const dhara_params *p, const oracle_olf_io *io);
 
 #ifdef __cplusplus
 }

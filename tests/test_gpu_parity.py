@@ -224,3 +224,26 @@ def test_error_paths(gpu):
         s.upload("ksat", np.full(d.ncells, np.nan))
     assert e.value.code == 5
     s.close()
+
+
+def _golden():
+    import json
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    with open(os.path.join(here, "manifest.json")) as f:
+        return here, json.load(f)["cases"]
+
+
+@pytest.mark.parametrize("precision", [db.FP64, db.MIXED])
+@pytest.mark.parametrize("case", _golden()[1], ids=lambda c: c["name"])
+def test_gpu_against_golden(gpu, case, precision):
+    """The CUDA path against the committed golden vectors (FP64 oracle)."""
+    import os
+    here, _ = _golden()
+    data = np.load(os.path.join(here, case["file"]))
+    d = inputs.make_domain(**dict(case["domain"], precision=precision))
+    st, dg, _ = db.run(d, nsteps=case["nsteps"])
+    for k in ("psi", "theta", "waterelev"):
+        assert rel_err(st[k], data[k]) < 1e-8, k
+    assert rel_err(st["ponding"], data["ponding"]) < 1e-6
+    assert dg["picard_iters_total"] == int(data["picard_iters_total"])
