@@ -109,9 +109,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_cell_iter():
-    """DRAM bytes per cell per inner Krylov iteration measured by ncu on the
-    same kernel (profiles/krylov_traffic.json, written from an ncu capture)."""
+def ncu_traffic_ratio():
+    """DRAM bytes per algorithmic byte of k_krylov, measured by ncu over every
+    k_krylov launch of a short run of this workload (profiles/krylov_traffic.json);
+    the traffic of a timed launch is this ratio times its algorithmic bytes."""
     p = os.path.join(ROOT, "profiles", "krylov_traffic.json")
     try:
         with open(p) as f:
@@ -282,10 +283,10 @@ def run_ours(args, world, rank, local):
     # algorithmic bytes of the timed region only (the counter is cumulative
     # per handle and this handle was created fresh for the timed region)
     achieved = (kbytes / (kms / 1e3)) / 1e9 if kms > 0 else None
-    ncu = ncu_traffic_per_cell_iter()
+    ncu = ncu_traffic_ratio()
     traffic = None
-    if ncu and kn > 0 and kiters > 0:
-        traffic = ncu["dram_bytes_per_cell_iter"] * N * (kiters / kn)
+    if ncu and kn > 0 and ncu.get("workload") == f"mixed_{p.nx}x{p.ny}x{p.nz}":
+        traffic = ncu["dram_bytes_per_algorithmic_byte"] * kbytes / kn
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_krylov<float>",

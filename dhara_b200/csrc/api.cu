@@ -5,7 +5,7 @@
 // SubsurfaceFlowModel then OverlandFlowModel, src/device.cu:450-458) is a
 // fixed launch sequence with no host synchronisation:
 //   k_prologue; [k_assemble, k_krylov (persistent), k_picard_check] x maxiter;
-//   k_epilogue; k_olf_setup, k_olf_solve (persistent), k_olf_finish
+//   k_epilogue; k_olf_setup, k_olf_pcg (persistent), k_olf_finish
 // Domains whose Picard loop has converged skip the remaining iterations on the
 // device, so the sequence can be captured once into a CUDA graph and replayed.
 #include "internal.h"
@@ -54,6 +54,7 @@ struct dhara_handle {
     std::vector<dhara_params> params;
     std::vector<DomainDesc> hdom;
     std::vector<TileDesc> htiles;
+    std::vector<OlfSeg> hsegs;
     long long Ntot = 0, Ctot = 0, WEtot = 0, SNtot = 0;
     DevPtrs P{};
     LaunchCfg L{};
@@ -449,6 +450,23 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         for (int y0 = 0; y0 < p.ny; y0 += TILE_Y)
             for (int x0 = 0; x0 < p.nx; x0 += TILE_X) h->htiles.push_back({d, x0, y0, 0});
         D.tile_end = (int)h->htiles.size();
+        // overland segments: runs of up to OLF_SEG surface cells of this domain
+        {
+            const int first = (int)h->hsegs.size();
+            const int C2 = p.nx * p.ny;
+            const int nseg = (C2 + OLF_SEG - 1) / OLF_SEG;
+            for (int k = 0; k < nseg; ++k) {
+                OlfSeg sg;
+                std::memset(&sg, 0, sizeof(sg));
+                sg.begin = D.off2 + (long long)k * OLF_SEG;
+                sg.dom = d;
+                sg.l0 = k * OLF_SEG;
+                sg.count = std::min(OLF_SEG, C2 - k * OLF_SEG);
+                sg.first = first;
+                sg.nseg = nseg;
+                h->hsegs.push_back(sg);
+            }
+        }
         if (p.nz > h->nz_max) h->nz_max = p.nz;
         if (p.picard_maxiter > h->maxiter_picard) h->maxiter_picard = p.picard_maxiter;
     }
@@ -475,8 +493,13 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         P.D64 = (double *)P.D;
     }
     for (double **q : {&P.ztopo, &P.mann, &P.h, &P.H, &P.ph, &P.ppt, &P.esoil, &P.tr, &P.hpoten, &P.qtop,
-                       &P.ktop, &P.bcqb, &P.olf_b, &P.olf_r, &P.olf_p0, &P.olf_p1, &P.olf_z})
+                       &P.ktop, &P.bcqb, &P.olf_b, &P.olf_r, &P.olf_p0, &P.olf_p1, &P.olf_z, &P.olf_w,
+                       &P.olf_s, &P.olf_p})
         rc |= dalloc(h, q, C);
+    OlfSeg *d_oseg = nullptr;
+    rc |= dalloc(h, &d_oseg, h->hsegs.size());
+    rc |= dalloc(h, &P.osst, h->hsegs.size());
+    rc |= dalloc(h, &P.olf_part, 7 * h->hsegs.size());
     rc |= dalloc(h, &P.olf_k, 4 * C);
     rc |= dalloc(h, &P.bcqw, (size_t)h->WEtot);
     rc |= dalloc(h, &P.bcqe, (size_t)h->WEtot);
@@ -498,6 +521,8 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     if (rc) return bail(DHARA_ERR_NOMEM);
     P.dom = h->d_dom;
     P.tiles = d_tiles;
+    P.oseg = d_oseg;
+    P.nseg = (int)h->hsegs.size();
     P.ntiles = (int)h->htiles.size();
     P.ndom = ndomains;
     P.smem_nz = h->nz_max;
@@ -514,8 +539,13 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     for (void *q : {P.K, P.D, P.r, P.p0, P.p1, P.z, P.d, P.q, P.finv, P.fe, P.fc}) e = e ? e : zero(q, N * sT);
     for (double *q : {P.K64, P.D64}) e = e ? e : zero(q, N * 8);
     for (double *q : {P.ztopo, P.mann, P.h, P.H, P.ph, P.ppt, P.esoil, P.tr, P.hpoten, P.qtop, P.ktop, P.bcqb,
-                      P.olf_b, P.olf_r, P.olf_p0, P.olf_p1, P.olf_z})
+                      P.olf_b, P.olf_r, P.olf_p0, P.olf_p1, P.olf_z, P.olf_w, P.olf_s, P.olf_p})
         e = e ? e : zero(q, C * 8);
+    e = e ? e : zero(P.osst, h->hsegs.size() * sizeof(OlfSegState));
+    e = e ? e : zero(P.olf_part, 7 * h->hsegs.size() * 8);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_oseg, h->hsegs.data(), sizeof(OlfSeg) * h->hsegs.size(), cudaMemcpyHostToDevice,
+                            h->stream);
     e = e ? e : zero(P.olf_k, 4 * C * 8);
     e = e ? e : zero(P.bcqw, (size_t)h->WEtot * 8);
     e = e ? e : zero(P.bcqe, (size_t)h->WEtot * 8);

@@ -87,6 +87,32 @@ struct OverlandCtrl {
     int active, iter, parity, pad;
 };
 
+// The overland solve works on segments: up to OLF_SEG consecutive surface
+// cells of one domain, one segment per block at a time, OLF_CPT cells per
+// thread.  A domain's segments are consecutive in the segment list.
+#define OLF_SEG 1024
+#define OLF_THREADS 256
+#define OLF_CPT (OLF_SEG / OLF_THREADS)
+// per-cell vectors kept in shared memory when every segment has its own block
+enum { OV_X, OV_R, OV_W, OV_Z, OV_S, OV_P, OV_M, OV_CW, OV_CE, OV_CS, OV_CN, OV_DG, OV_N };
+
+struct OlfSeg {
+    long long begin;  // global surface index of the first cell
+    int dom;
+    int l0;           // index of the first cell within its domain
+    int count;        // cells in the segment
+    int first;        // index of the domain's first segment
+    int nseg;         // segments of the domain
+    int pad;
+};
+
+// Scalars of the pipelined CG recurrence for one segment.  Every segment of a
+// domain computes the same values from the same domain sums.
+struct OlfSegState {
+    double gamma_prev, alpha_prev, bb;
+    int iter, active;
+};
+
 // Diagnostics accumulated on the device (copied into dhara_diagnostics).
 struct DevDiag {
     long long picard_iters_total, krylov_iters_total, refine_iters_total, overland_iters_total;
@@ -109,6 +135,7 @@ struct GlobalCtrl {
     int n_inner_active;  // domains with an active inner solve
     int n_olf_active;
     int pad;
+    int olf_live[4];     // domains still iterating, rotating over three phases
 };
 
 // Number of double partial sums per tile kept for reductions.
@@ -135,6 +162,11 @@ struct DevPtrs {
     double *ztopo, *mann, *h, *H, *ph, *ppt, *esoil, *tr, *hpoten, *qtop, *ktop, *bcqb;
     double *olf_k;       // 4*C: kw, ke, ks, kn per column (row-based)
     double *olf_b, *olf_r, *olf_p0, *olf_p1, *olf_z;
+    double *olf_w, *olf_s, *olf_p;
+    const OlfSeg *oseg;  // [nseg]
+    OlfSegState *osst;   // [nseg]
+    double *olf_part;    // [2][3][nseg] recurrence sums + [nseg] ||b||^2 partials
+    int nseg, pad_seg;
     // faces
     double *bcqw, *bcqe, *bcqs, *bcqn;
     int *procmap;
@@ -158,6 +190,8 @@ struct DevPtrs {
 struct LaunchCfg {
     int coop_blocks_3d;   // resident blocks for the persistent 3D solve
     int coop_blocks_2d;
+    int olf_res_blocks;    // co-resident blocks of the shared-memory-resident overland solve
+    int olf_stream_blocks; // co-resident blocks of the streaming overland solve
     int smem_3d;          // dynamic shared memory bytes of the 3D solve
     int nz_max;
     int mixed;

@@ -3,7 +3,7 @@
 //
 //   WaterElevationOverland (33-45) + UpdateKOverland (193-368)
 //     + SetUpLinearSystemsOverland (65-189)                  -> k_olf_setup
-//   CUSP CG on the 5-diagonal matrix (410-411)               -> k_olf_solve
+//   CUSP CG on the 5-diagonal matrix (410-411)               -> k_olf_pcg
 //   WaterDepthOverland (371-383) + ph <- waterdepth (417)     -> k_olf_finish
 //
 // The boundary ring is a fixed-elevation (identity) row in the reference.  Its
@@ -34,11 +34,14 @@ __global__ void __launch_bounds__(TILE_THREADS) k_olf_setup(DevPtrs P, long long
     const DomainDesc &D = P.dom[td.dom];
     if (threadIdx.x == 0 && tile == D.tile_begin) {
         OverlandCtrl &oc = P.octrl[td.dom];
-        oc.active = 1;
         oc.iter = 0;
-        oc.parity = 0;
-        oc.pad = 1;  // first inner iteration
-        atomicAdd(&P.gctrl->n_olf_active, 1);
+        oc.rr = 0.0;
+        oc.bb = 0.0;
+    }
+    if (threadIdx.x == 0 && tile == 0) {
+        P.gctrl->olf_live[0] = 0;
+        P.gctrl->olf_live[1] = 0;
+        P.gctrl->olf_live[2] = 0;
     }
     const ColumnRef cr = column_of(P, tile);
     if (!cr.valid) return;
@@ -104,115 +107,323 @@ __device__ __forceinline__ double olf_apply(const OlfRow &w, const ColumnRef &cr
            w.cy * (w.kn * (c - v(I + cr.nx)) + w.ks * (c - v(I - cr.nx)));
 }
 
-// Persistent cooperative Jacobi-PCG over all domains' interior cells.
-__global__ void __launch_bounds__(TILE_THREADS) k_olf_solve(DevPtrs P, long long ctot) {
-    double *x = P.H, *r = P.olf_r, *z = P.olf_z;
-    // R: r = b - A x, z = r / diag
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const int dom = P.tiles[t].dom;
-        if (!ldcg(&P.octrl[dom].active)) continue;
-        const ColumnRef cr = column_of(P, t);
-        const DomainDesc &D = P.dom[dom];
-        double v[3] = {0, 0, 0};  // rr, bb, rz
-        if (cr.valid) {
-            const double bI = P.olf_b[cr.c];
-            v[1] = bI * bI;
-            const OlfRow w = olf_row(P, cr, D, ctot);
-            double rI = 0.0, zI = 0.0;
-            if (!w.ring) {
-                rI = bI - olf_apply(w, cr, [&](long long q) { return x[q]; });
-                zI = rI / w.diag;
+// ------------------------------------------------------------------ solve
+// Pipelined Jacobi-preconditioned CG (Ghysels & Vanroose 2014, Alg. 4) over
+// the interior cells of every domain, in one persistent cooperative launch.
+// The recurrence needs one inner-product pair (gamma = r.u, delta = w.u) per
+// iteration, and its partial sums are written in the same phase as the
+// preconditioned vector m = w/diag that the next matrix product reads, so one
+// grid barrier per iteration makes both visible.  After the barrier every
+// block sums its domains' per-segment partials itself, in the same order in
+// every block, so all blocks see bitwise identical scalars without a second
+// barrier.  The fixed ring is eliminated (its values stay H_old).
+//
+// Vectors: x (= H), r, w = A u, z = A q, s = A p, p, with u = r/diag and
+// q = s/diag formed on the fly; m alternates between two buffers.  In the
+// resident variant (RES) each block owns one segment for the whole solve and
+// keeps x, r, w, z, s, p, m and the row coefficients in shared memory; only m
+// goes through global memory (for the neighbours) and x is written back when
+// the domain stops.
+
+template <int NV>
+__device__ __forceinline__ void olf_block_sum(double (&v)[NV]) {
+    __shared__ double s_w[NV][OLF_THREADS / 32];
+    __shared__ double s_out[NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        double a = v[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) s_w[i][warp] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double a = 0.0;
+#pragma unroll
+        for (int w = 0; w < OLF_THREADS / 32; ++w) a += s_w[threadIdx.x][w];
+        s_out[threadIdx.x] = a;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = s_out[i];
+    __syncthreads();
+}
+
+// Domain totals of per-segment partials (component-major: part[i*nseg + s]).
+template <int NV>
+__device__ __forceinline__ void olf_domain_sum(const double *part, int nseg_tot, int first, int nseg,
+                                               double (&v)[NV]) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = 0.0;
+    for (int k = threadIdx.x; k < nseg; k += OLF_THREADS) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] += __ldcg(&part[(size_t)i * nseg_tot + first + k]);
+    }
+    olf_block_sum<NV>(v);
+}
+
+struct OlfCell {
+    long long c;
+    int nx;
+    bool live, ring;
+};
+
+__device__ __forceinline__ OlfCell olf_cell(const OlfSeg &sg, const DomainDesc &D, int t) {
+    OlfCell q;
+    q.live = t < sg.count;
+    const int l = sg.l0 + t;
+    const int j = l / D.nx, i = l - j * D.nx;
+    q.c = sg.begin + t;
+    q.nx = D.nx;
+    q.ring = is_ring(i, j, D.nx, D.ny);
+    return q;
+}
+
+// 5-point product of the interior row at c: diag*v_c - sum of the scaled
+// conductances times the neighbours (row-owned kw, ke, ks, kn as the
+// reference's SetUpLinearSystemsOverland builds them).
+struct OlfCoef {
+    double cw, ce, cs, cn, dg;
+};
+
+__device__ __forceinline__ OlfCoef olf_coef(const DevPtrs &P, const DomainDesc &D, long long c, long long ctot) {
+    const double cx = D.dt / (D.dx * D.dx), cy = D.dt / (D.dy * D.dy);
+    OlfCoef k;
+    k.cw = cx * P.olf_k[0 * ctot + c];
+    k.ce = cx * P.olf_k[1 * ctot + c];
+    k.cs = cy * P.olf_k[2 * ctot + c];
+    k.cn = cy * P.olf_k[3 * ctot + c];
+    k.dg = 1.0 + (k.ce + k.cw) + (k.cn + k.cs);
+    return k;
+}
+
+template <bool CG>
+__device__ __forceinline__ double olf_av(const OlfCoef &k, const double *v, long long c, int nx, double vc) {
+    const double vw = CG ? __ldcg(v + c - 1) : v[c - 1];
+    const double ve = CG ? __ldcg(v + c + 1) : v[c + 1];
+    const double vs = CG ? __ldcg(v + c - nx) : v[c - nx];
+    const double vn = CG ? __ldcg(v + c + nx) : v[c + nx];
+    return k.dg * vc - ((k.ce * ve + k.cw * vw) + (k.cn * vn + k.cs * vs));
+}
+
+template <bool RES>
+__global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ctot) {
+    extern __shared__ double s_res[];  // RES: [OV_N][OLF_SEG]
+    __shared__ double s_ab[2];
+    __shared__ int s_go;
+    const int S = P.nseg;
+    const int tid = threadIdx.x;
+    const int s_lo = (int)(((long long)blockIdx.x * S) / gridDim.x);
+    const int s_hi = (int)(((long long)(blockIdx.x + 1) * S) / gridDim.x);
+    double *const mbuf0 = P.olf_p0, *const mbuf1 = P.olf_p1;
+    double *part = P.olf_part;
+    double *bbp = P.olf_part + (size_t)6 * S;
+    auto sv = [&](int v, int t) -> double & { return s_res[v * OLF_SEG + t]; };
+
+    // ---- r = b - A x, u = r/diag (into m buffer 0), ||b||^2 partials
+    for (int s = s_lo; s < s_hi; ++s) {
+        const OlfSeg sg = P.oseg[s];
+        const DomainDesc &D = P.dom[sg.dom];
+        double v[1] = {0.0};
+#pragma unroll
+        for (int k = 0; k < OLF_CPT; ++k) {
+            const int t = tid + k * OLF_THREADS;
+            const OlfCell q = olf_cell(sg, D, t);
+            if (!q.live) continue;
+            const double bI = P.olf_b[q.c];
+            v[0] += bI * bI;
+            double r = 0.0, u = 0.0;
+            const double xc = P.H[q.c];
+            OlfCoef cf{0, 0, 0, 0, 1.0};
+            if (!q.ring) {
+                cf = olf_coef(P, D, q.c, ctot);
+                r = bI - olf_av<false>(cf, P.H, q.c, q.nx, xc);
+                u = r / cf.dg;
             }
-            r[cr.c] = rI;
-            z[cr.c] = zI;
-            v[0] = rI * rI;
-            v[2] = rI * zI;
+            mbuf0[q.c] = u;
+            if (RES) {
+                sv(OV_X, t) = xc; sv(OV_R, t) = r;
+                sv(OV_CW, t) = cf.cw; sv(OV_CE, t) = cf.ce; sv(OV_CS, t) = cf.cs; sv(OV_CN, t) = cf.cn;
+                sv(OV_DG, t) = cf.dg;
+            } else {
+                P.olf_r[q.c] = r;
+            }
         }
-        if (domain_reduce<3>(P, t, dom, 3, v) && threadIdx.x == 0) {
-            OverlandCtrl &c = P.octrl[dom];
-            c.bb = v[1];
-            c.rr = v[0];
-            c.rz = v[2];
-            const double tol2 = D.overland_tol * D.overland_tol;
-            if (v[0] <= tol2 * v[1] || c.iter >= D.overland_maxiter || !(v[0] == v[0])) {
-                c.active = 0;
-                atomicSub(&P.gctrl->n_olf_active, 1);
-            }
+        olf_block_sum<1>(v);
+        if (tid == 0) {
+            __stcg(&bbp[s], v[0]);
+            OlfSegState st;
+            st.gamma_prev = 0.0; st.alpha_prev = 0.0; st.bb = 0.0; st.iter = 0; st.active = 1;
+            P.osst[s] = st;
         }
     }
     if (!grid_sync(P.barrier)) return;
-    while (ldcg(&P.gctrl->n_olf_active) > 0) {
-        // A: p = z + beta p_old, partial p.Ap
-        for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-            const int dom = P.tiles[t].dom;
-            const OverlandCtrl *oc = &P.octrl[dom];
-            if (!ldcg(&oc->active)) continue;
-            const ColumnRef cr = column_of(P, t);
-            const DomainDesc &D = P.dom[dom];
-            const int parity = ldcg(&oc->parity);
-            const bool first = ldcg(&oc->pad) != 0;
-            const double beta = ldcg(&oc->beta);
-            const double *pold = parity ? P.olf_p1 : P.olf_p0;
-            double *pnew = parity ? P.olf_p0 : P.olf_p1;
-            double v[1] = {0};
-            if (cr.valid) {
-                const OlfRow w = olf_row(P, cr, D, ctot);
-                auto pv = [&](long long q) { return first ? z[q] : z[q] + beta * pold[q]; };
-                const double pI = w.ring ? 0.0 : pv(cr.c);
-                if (!w.ring) v[0] = pI * olf_apply(w, cr, pv);
-                pnew[cr.c] = pI;
+
+    // ---- w = A u, m_0 = w/diag (into m buffer 1), sums of iteration 0
+    for (int s = s_lo; s < s_hi; ++s) {
+        const OlfSeg sg = P.oseg[s];
+        const DomainDesc &D = P.dom[sg.dom];
+        double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < OLF_CPT; ++k) {
+            const int t = tid + k * OLF_THREADS;
+            const OlfCell q = olf_cell(sg, D, t);
+            if (!q.live) continue;
+            double w = 0.0, m = 0.0;
+            if (!q.ring) {
+                const OlfCoef cf = RES ? OlfCoef{sv(OV_CW, t), sv(OV_CE, t), sv(OV_CS, t), sv(OV_CN, t), sv(OV_DG, t)}
+                                       : olf_coef(P, D, q.c, ctot);
+                const double u = __ldcg(mbuf0 + q.c);
+                const double r = RES ? sv(OV_R, t) : P.olf_r[q.c];
+                w = olf_av<true>(cf, mbuf0, q.c, q.nx, u);
+                m = w / cf.dg;
+                v[0] += r * u;
+                v[1] += w * u;
+                v[2] += r * r;
             }
-            if (domain_reduce<1>(P, t, dom, 3, v) && threadIdx.x == 0) {
-                OverlandCtrl &c = P.octrl[dom];
-                c.pAp = v[0];
-                c.alpha = c.rz / v[0];
-                c.parity ^= 1;
-                if (!(v[0] > 0.0)) {
-                    c.active = 0;
-                    atomicSub(&P.gctrl->n_olf_active, 1);
-                }
-            }
-        }
-        if (!grid_sync(P.barrier)) return;
-        // B: x += alpha p, r -= alpha A p, z = r / diag
-        for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-            const int dom = P.tiles[t].dom;
-            const OverlandCtrl *oc = &P.octrl[dom];
-            if (!ldcg(&oc->active)) continue;
-            const ColumnRef cr = column_of(P, t);
-            const DomainDesc &D = P.dom[dom];
-            const int parity = ldcg(&oc->parity);
-            const double alpha = ldcg(&oc->alpha);
-            const double *p = parity ? P.olf_p1 : P.olf_p0;
-            double v[2] = {0, 0};
-            if (cr.valid) {
-                const OlfRow w = olf_row(P, cr, D, ctot);
-                if (!w.ring) {
-                    const double Ap = olf_apply(w, cr, [&](long long q) { return p[q]; });
-                    x[cr.c] += alpha * p[cr.c];
-                    const double rI = r[cr.c] - alpha * Ap;
-                    const double zI = rI / w.diag;
-                    r[cr.c] = rI;
-                    z[cr.c] = zI;
-                    v[0] = rI * rI;
-                    v[1] = rI * zI;
-                }
-            }
-            if (domain_reduce<2>(P, t, dom, 3, v) && threadIdx.x == 0) {
-                OverlandCtrl &c = P.octrl[dom];
-                c.rr = v[0];
-                c.beta = v[1] / c.rz;
-                c.rz = v[1];
-                c.pad = 0;
-                c.iter += 1;
-                const double tol2 = D.overland_tol * D.overland_tol;
-                if (v[0] <= tol2 * c.bb || c.iter >= D.overland_maxiter || !(v[0] == v[0])) {
-                    c.active = 0;
-                    atomicSub(&P.gctrl->n_olf_active, 1);
-                }
+            mbuf1[q.c] = m;
+            if (RES) {
+                sv(OV_W, t) = w;
+                sv(OV_M, t) = m;
+            } else {
+                P.olf_w[q.c] = w;
             }
         }
+        olf_block_sum<3>(v);
+        if (tid == 0) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) __stcg(&part[(size_t)i * S + s], v[i]);
+        }
+    }
+    if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[2] = 0;
+    if (!grid_sync(P.barrier)) return;
+
+    // ---- iterations
+    for (int it = 0;; ++it) {
+        const double *pin = part + (size_t)(it & 1) * 3 * S;
+        double *pout = part + (size_t)((it + 1) & 1) * 3 * S;
+        const double *mcur = (it & 1) ? mbuf0 : mbuf1;
+        double *mnext = (it & 1) ? mbuf1 : mbuf0;
+        int prev_dom = -1;
+        double dsum[3] = {0.0, 0.0, 0.0};
+        for (int s = s_lo; s < s_hi; ++s) {
+            const OlfSeg sg = P.oseg[s];
+            const DomainDesc &D = P.dom[sg.dom];
+            if (sg.dom != prev_dom) {
+                olf_domain_sum<3>(pin, S, sg.first, sg.nseg, dsum);
+                prev_dom = sg.dom;
+            }
+            double bbd[1] = {0.0};
+            if (it == 0) olf_domain_sum<1>(bbp, S, sg.first, sg.nseg, bbd);
+            bool stopped_now = false;
+            if (tid == 0) {
+                OlfSegState st = P.osst[s];
+                if (it == 0) st.bb = bbd[0];
+                int go = 0;
+                if (st.active) {
+                    const double gam = dsum[0], del = dsum[1], rr = dsum[2];
+                    const double tol2 = D.overland_tol * D.overland_tol;
+                    bool stop = rr <= tol2 * st.bb;
+                    stop = stop || it >= D.overland_maxiter || !(rr == rr) || !(gam == gam);
+                    double alpha = 0.0, beta = 0.0;
+                    if (!stop) {
+                        if (it == 0) {
+                            alpha = gam / del;
+                        } else {
+                            beta = gam / st.gamma_prev;
+                            alpha = gam / (del - beta * gam / st.alpha_prev);
+                        }
+                        if (!(alpha > 0.0) || !(alpha < 1e300)) stop = true;  // breakdown
+                    }
+                    if (stop) {
+                        st.active = 0;
+                        stopped_now = true;
+                        if (s == sg.first) {
+                            OverlandCtrl &oc = P.octrl[sg.dom];
+                            oc.iter = it;
+                            oc.rr = rr;
+                            oc.bb = st.bb;
+                        }
+                    } else {
+                        st.gamma_prev = gam;
+                        st.alpha_prev = alpha;
+                        st.iter = it + 1;
+                        go = 1;
+                        if (s == sg.first) atomicAdd(&P.gctrl->olf_live[(it + 1) % 3], 1);
+                        s_ab[0] = alpha;
+                        s_ab[1] = beta;
+                    }
+                    P.osst[s] = st;
+                }
+                s_go = go | (stopped_now ? 2 : 0);
+            }
+            __syncthreads();
+            const int go = s_go;
+            const double alpha = s_ab[0], beta = s_ab[1];
+            __syncthreads();
+            if (!(go & 1)) {
+                if (RES && (go & 2)) {
+#pragma unroll
+                    for (int k = 0; k < OLF_CPT; ++k) {
+                        const int t = tid + k * OLF_THREADS;
+                        if (t < sg.count) P.H[sg.begin + t] = sv(OV_X, t);
+                    }
+                }
+                continue;
+            }
+            const bool first = it == 0;
+            double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < OLF_CPT; ++k) {
+                const int t = tid + k * OLF_THREADS;
+                const OlfCell q = olf_cell(sg, D, t);
+                if (!q.live || q.ring) continue;
+                const long long c = q.c;
+                const OlfCoef cf = RES ? OlfCoef{sv(OV_CW, t), sv(OV_CE, t), sv(OV_CS, t), sv(OV_CN, t), sv(OV_DG, t)}
+                                       : olf_coef(P, D, c, ctot);
+                const double mc = RES ? sv(OV_M, t) : __ldcg(mcur + c);
+                const double n = olf_av<true>(cf, mcur, c, q.nx, mc);
+                double r = RES ? sv(OV_R, t) : P.olf_r[c];
+                double w = RES ? sv(OV_W, t) : P.olf_w[c];
+                double x = RES ? sv(OV_X, t) : P.H[c];
+                double z, sdir, p;
+                const double u = r / cf.dg;
+                if (first) {
+                    z = n;
+                    sdir = w;
+                    p = u;
+                } else {
+                    z = n + beta * (RES ? sv(OV_Z, t) : P.olf_z[c]);
+                    sdir = w + beta * (RES ? sv(OV_S, t) : P.olf_s[c]);
+                    p = u + beta * (RES ? sv(OV_P, t) : P.olf_p[c]);
+                }
+                x += alpha * p;
+                r -= alpha * sdir;
+                w -= alpha * z;
+                const double un = r / cf.dg;
+                const double mn = w / cf.dg;
+                v[0] += r * un;
+                v[1] += w * un;
+                v[2] += r * r;
+                mnext[c] = mn;
+                if (RES) {
+                    sv(OV_Z, t) = z; sv(OV_S, t) = sdir; sv(OV_P, t) = p;
+                    sv(OV_X, t) = x; sv(OV_R, t) = r; sv(OV_W, t) = w; sv(OV_M, t) = mn;
+                } else {
+                    P.olf_z[c] = z; P.olf_s[c] = sdir; P.olf_p[c] = p;
+                    P.H[c] = x; P.olf_r[c] = r; P.olf_w[c] = w;
+                }
+            }
+            olf_block_sum<3>(v);
+            if (tid == 0) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) __stcg(&pout[(size_t)i * S + s], v[i]);
+            }
+        }
+        if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
         if (!grid_sync(P.barrier)) return;
+        if (__ldcg(&P.gctrl->olf_live[(it + 1) % 3]) == 0) break;
     }
 }
 
@@ -260,13 +471,17 @@ cudaError_t launch_overland_setup(const DevPtrs &P, long long ctot, cudaStream_t
     return cudaGetLastError();
 }
 
+#define OLF_RES_SMEM (OV_N * OLF_SEG * (int)sizeof(double))
+
 cudaError_t launch_overland_solve(const DevPtrs &P, const LaunchCfg &L, long long ctot, cudaStream_t s) {
     DevPtrs args = P;
     long long c = ctot;
     void *kargs[] = {&args, &c};
-    const int grid = L.coop_blocks_2d < P.ntiles ? L.coop_blocks_2d : P.ntiles;
-    return cudaLaunchCooperativeKernel((const void *)k_olf_solve, dim3(grid), dim3(TILE_THREADS), kargs, 0,
-                                       s);
+    if (P.nseg <= L.olf_res_blocks)
+        return cudaLaunchCooperativeKernel((const void *)k_olf_pcg<true>, dim3(P.nseg), dim3(OLF_THREADS), kargs,
+                                           OLF_RES_SMEM, s);
+    const int grid = L.olf_stream_blocks < P.nseg ? L.olf_stream_blocks : P.nseg;
+    return cudaLaunchCooperativeKernel((const void *)k_olf_pcg<false>, dim3(grid), dim3(OLF_THREADS), kargs, 0, s);
 }
 
 cudaError_t launch_overland_finish(const DevPtrs &P, long long ctot, cudaStream_t s) {
@@ -278,10 +493,18 @@ cudaError_t configure_2d(LaunchCfg &L, int device) {
     cudaDeviceProp prop;
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute((const void *)k_olf_pcg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             OLF_RES_SMEM);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_solve, TILE_THREADS, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_pcg<true>, OLF_THREADS,
+                                                      OLF_RES_SMEM);
+    if (e != cudaSuccess) return e;
+    L.olf_res_blocks = per_sm * prop.multiProcessorCount;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_pcg<false>, OLF_THREADS, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    L.coop_blocks_2d = per_sm * prop.multiProcessorCount;
+    L.olf_stream_blocks = per_sm * prop.multiProcessorCount;
+    L.coop_blocks_2d = L.olf_stream_blocks;
     return cudaSuccess;
 }

@@ -28,6 +28,14 @@ static void ref_down(T *h, const RefBuf &b, size_t count) {
     if (h) cudaMemcpy(h, b.p, count * sizeof(T), cudaMemcpyDeviceToHost);
 }
 
+// Copy back from a device pointer returned by ref_up (the safer form: the
+// pointer names the buffer, so no index can pick the wrong one).
+template <typename T>
+static int ref_down_ptr(T *h, const T *d, size_t count) {
+    if (!h) return 0;
+    return cudaMemcpy(h, d, count * sizeof(T), cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : 1;
+}
+
 // The reference's __constant__ physics (include/devconst.h), set from the
 // runtime parameters in the reference's units (alpha in 1/cm).  Expanded in
 // each launcher file because each reference .cu has its own copies.

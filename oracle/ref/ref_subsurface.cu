@@ -36,10 +36,10 @@ extern "C" int ref_k_assemble(const dhara_params *p, const oracle_asm_io *io) {
         a3d, rhs, pm, pn, tm, tn, km, cm, wbc, ebc, sbc, nbc, tbc, bbc, pw, pe, pss, pnn, pt, pb, qw, qe, qs, qn,
         qt, qb, tr, pm2, root, make_int3(io->nx, io->ny, io->nz));
     if (cudaDeviceSynchronize() != cudaSuccess) return 1;
-    ref_down(io->a3d, b[0], 7 * N);
-    ref_down(io->rhs, b[1], N);
-    ref_down(io->qb, b[23], Cc);
-    return 0;
+    int rc = ref_down_ptr(io->a3d, a3d, 7 * N);
+    rc |= ref_down_ptr(io->rhs, rhs, N);
+    rc |= ref_down_ptr(io->qb, qb, Cc);
+    return rc;
 }
 
 extern "C" int ref_k_infiltration(const dhara_params *p, const oracle_top_io *io) {
