@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdhara_b200.so")
 
 KERNELS = {"krylov": 0, "assemble": 1, "picard_check": 2, "epilogue": 3, "overland_solve": 4,
-           "overland_aux": 5, "prologue": 6}
+           "overland_aux": 5, "prologue": 6, "adjoint": 7}
 
 _lib = None
 
@@ -66,6 +66,7 @@ def lib():
         "dhara_reset_kernel_timing": (ct.c_int, [vp]),
         "dhara_get_launch_count": (ct.c_int, [vp, i64p]),
         "dhara_get_krylov_traffic": (ct.c_int, [vp, dp, i64p]),
+        "dhara_adjoint": (ct.c_int, [vp, P(_abi.AdjointDesc), dp, dp, dp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -200,6 +201,28 @@ class Solver:
         n = ct.c_int64()
         _check(lib().dhara_get_launch_count(self.h, ct.byref(n)))
         return n.value
+
+    def adjoint(self, theta_target, q_target, nsteps, checkpoint_every=10, w_q=1.0, gradients=True):
+        """Runs nsteps from the current state and returns the loss (and, with
+        gradients, dL/dlog Ks, dL/dalpha, dL/dn in the reference 3D layout) of
+        the theta / outflow misfit; see dhara_adjoint in include/dhara_gpu.h."""
+        p = self.params[0]
+        C, N = p.nx * p.ny, p.nx * p.ny * p.nz
+        th = np.ascontiguousarray(theta_target, dtype=np.float64).reshape(-1)
+        q = np.ascontiguousarray(q_target, dtype=np.float64).reshape(-1)
+        if th.size != nsteps * 3 * C or q.size != nsteps:
+            raise ValueError("targets must be [nsteps][3][nx*ny] and [nsteps]")
+        d = _abi.AdjointDesc()
+        d.struct_size = ct.sizeof(_abi.AdjointDesc)
+        d.nsteps, d.checkpoint_every, d.w_q = nsteps, checkpoint_every, w_q
+        d.theta_target, d.q_target = _dp(th), _dp(q)
+        loss = ct.c_double()
+        if gradients:
+            g = [np.zeros(N) for _ in range(3)]
+            _check(lib().dhara_adjoint(self.h, ct.byref(d), ct.byref(loss), *[_dp(a) for a in g]))
+            return loss.value, g[0], g[1], g[2]
+        _check(lib().dhara_adjoint(self.h, ct.byref(d), ct.byref(loss), None, None, None))
+        return loss.value
 
     def krylov_traffic(self):
         b = ct.c_double()

@@ -72,6 +72,14 @@ class Diagnostics(ct.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
+class AdjointDesc(ct.Structure):
+    _fields_ = [
+        ("struct_size", ct.c_int32), ("nsteps", ct.c_int32), ("checkpoint_every", ct.c_int32),
+        ("pad", ct.c_int32), ("theta_target", ct.POINTER(ct.c_double)), ("q_target", ct.POINTER(ct.c_double)),
+        ("w_q", ct.c_double), ("reserved", ct.c_double * 4),
+    ]
+
+
 def make_params(nx, ny, nz, dx=1.0, dy=1.0, dz=0.05, dt=60.0, **kw):
     """Parameters with the reference's device defaults (include/devconst.h:6-31,
     converted to SI: alpha 0.02 /cm -> 2.0 /m, dt in seconds) overridden by kw."""

@@ -40,7 +40,7 @@ int fail(int code, const char *fmt, ...) {
             return fail(DHARA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
     } while (0)
 
-enum { KT_KRYLOV = 0, KT_ASSEMBLE, KT_CHECK, KT_EPILOGUE, KT_OLF_SOLVE, KT_OLF_AUX, KT_PROLOGUE, KT_N };
+enum { KT_KRYLOV = 0, KT_ASSEMBLE, KT_CHECK, KT_EPILOGUE, KT_OLF_SOLVE, KT_OLF_AUX, KT_PROLOGUE, KT_ADJOINT, KT_N };
 
 }  // namespace
 
@@ -76,6 +76,7 @@ struct dhara_handle {
     double total_ms[KT_N] = {};
     long long launches[KT_N] = {};
     long long launch_count = 0;
+    std::vector<int> adj_step_host;  // step counters uploaded by the adjoint sweep
 };
 
 namespace {
@@ -186,13 +187,20 @@ void collect_timing(dhara_handle *h) {
             return fail(DHARA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));       \
     } while (0)
 
-int enqueue_subsurface(dhara_handle *h) {
+// With a tape (the adjoint's recompute sweep), every Picard iterate psi^m and
+// solution x^m is copied into the tape slot after its solve.
+int enqueue_subsurface(dhara_handle *h, const AdjPtrs *tape = nullptr, int slot = 0) {
     const DevPtrs &P = h->P;
     cudaStream_t s = h->stream;
     LAUNCH(KT_PROLOGUE, launch_prologue(P, s));
     for (int m = 0; m < h->maxiter_picard; ++m) {
         LAUNCH(KT_ASSEMBLE, launch_assemble(P, h->L, s));
         LAUNCH(KT_KRYLOV, launch_krylov(P, h->L, s));
+        if (tape) {
+            const size_t off = ((size_t)slot * tape->maxiter + m) * tape->np;
+            CK(cudaMemcpyAsync(tape->t_psim + off, P.psim, tape->np * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(tape->t_xm + off, P.x, tape->np * 8, cudaMemcpyDeviceToDevice, s));
+        }
         LAUNCH(KT_CHECK, launch_picard_check(P, s));
     }
     LAUNCH(KT_EPILOGUE, launch_epilogue(P, h->L, s));
@@ -984,3 +992,278 @@ int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ adjoint
+namespace {
+
+struct DevScratch {
+    std::vector<void *> ptrs;
+    ~DevScratch() {
+        for (void *p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    int get(T **p, size_t count) {
+        void *q = nullptr;
+        if (cudaMalloc(&q, (count ? count : 1) * sizeof(T)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(DHARA_ERR_NOMEM, "adjoint: cudaMalloc of %zu bytes failed", count * sizeof(T));
+        }
+        ptrs.push_back(q);
+        *p = (T *)q;
+        return DHARA_OK;
+    }
+};
+
+// The state a step starts from: psi^n, theta^n, K(psi^n) of the top layer,
+// the ponded depth (= overland depth) and the step counter.  The Krylov warm
+// start equals psi^n and the overland elevation is rebuilt from the depth.
+struct StateCopy {
+    double *psin, *thetan, *ktop, *ph, *h, *H;
+};
+
+int copy_state(dhara_handle *h, const StateCopy &dst, bool to_handle, int step) {
+    const DevPtrs &P = h->P;
+    const size_t np = (size_t)h->Ntot * 8, nc = (size_t)h->Ctot * 8;
+    cudaStream_t s = h->stream;
+    auto cp = [&](double *handle_arr, double *copy, size_t bytes) {
+        return to_handle ? cudaMemcpyAsync(handle_arr, copy, bytes, cudaMemcpyDeviceToDevice, s)
+                         : cudaMemcpyAsync(copy, handle_arr, bytes, cudaMemcpyDeviceToDevice, s);
+    };
+    CK(cp(P.psin, dst.psin, np));
+    CK(cp(P.thetan, dst.thetan, np));
+    CK(cp(P.ktop, dst.ktop, nc));
+    CK(cp(P.ph, dst.ph, nc));
+    CK(cp(P.h, dst.h, nc));
+    if (dst.H) CK(cp(P.H, dst.H, nc));
+    if (to_handle) {
+        CK(cudaMemcpyAsync(P.x, dst.psin, np, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(P.psim, dst.psin, np, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(&P.pctrl[0].step, &h->adj_step_host[step], sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+    return DHARA_OK;
+}
+
+}  // namespace
+
+int dhara_adjoint(dhara_handle *h, const dhara_adjoint_desc *desc, double *loss, double *grad_logks,
+                  double *grad_alpha, double *grad_n) {
+    if (!h || !desc || !loss) return fail(DHARA_ERR_INVALID, "NULL argument");
+    if (desc->struct_size != (int)sizeof(dhara_adjoint_desc))
+        return fail(DHARA_ERR_INVALID, "struct_size %d != sizeof(dhara_adjoint_desc) %d", desc->struct_size,
+                    (int)sizeof(dhara_adjoint_desc));
+    if (h->ndom != 1) return fail(DHARA_ERR_UNSUPPORTED, "the adjoint runs on single-domain handles");
+    if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
+    if (desc->nsteps < 1 || desc->checkpoint_every < 1 || !desc->theta_target || !desc->q_target)
+        return fail(DHARA_ERR_INVALID, "adjoint: need nsteps >= 1, checkpoint_every >= 1 and both targets");
+    const bool want_grad = grad_logks && grad_alpha && grad_n;
+    if (!want_grad && (grad_logks || grad_alpha || grad_n))
+        return fail(DHARA_ERR_INVALID, "adjoint: pass all three gradient arrays or none");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->graph_exec) {
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    const DevPtrs &P = h->P;
+    const DomainDesc &D = h->hdom[0];
+    cudaStream_t s = h->stream;
+    const int nsteps = desc->nsteps, K = desc->checkpoint_every;
+    const int nseg = (nsteps + K - 1) / K;
+    const int S = K < nsteps ? K : nsteps;
+    const size_t np = (size_t)h->Ntot, nc = (size_t)h->Ctot, C = (size_t)D.nx * D.ny;
+    const int M = h->maxiter_picard;
+
+    DevScratch mem;
+    AdjPtrs A;
+    std::memset(&A, 0, sizeof(A));
+    A.np = (long long)np;
+    A.nc = (long long)nc;
+    A.maxiter = M;
+    A.w_q = desc->w_q;
+    int rc = 0;
+    double *theta_target = nullptr, *q_target = nullptr;
+    rc |= mem.get(&theta_target, (size_t)nsteps * 3 * C);
+    rc |= mem.get(&q_target, (size_t)nsteps);
+    rc |= mem.get(&A.qhist, (size_t)nsteps);
+    rc |= mem.get(&A.q_prev, 1);
+    rc |= mem.get(&A.loss, 1);
+    std::vector<StateCopy> ckpt(nseg + 1);
+    for (int k = 0; k <= nseg && !rc; ++k) {
+        rc |= mem.get(&ckpt[k].psin, np);
+        rc |= mem.get(&ckpt[k].thetan, np);
+        rc |= mem.get(&ckpt[k].ktop, nc);
+        rc |= mem.get(&ckpt[k].ph, nc);
+        rc |= mem.get(&ckpt[k].h, nc);
+        ckpt[k].H = nullptr;
+    }
+    double *final_H = nullptr;
+    rc |= mem.get(&final_H, nc);
+    // the overland solution and depth of every step: the recompute sweep
+    // restores them instead of solving the overland system again
+    double *olf_H_all = nullptr, *olf_h_all = nullptr;
+    if (want_grad) {
+        rc |= mem.get(&olf_H_all, (size_t)nsteps * nc);
+        rc |= mem.get(&olf_h_all, (size_t)nsteps * nc);
+    }
+    if (rc) return DHARA_ERR_NOMEM;
+    A.theta_target = theta_target;
+    A.q_target = q_target;
+    CK(cudaMemcpyAsync(theta_target, desc->theta_target, (size_t)nsteps * 3 * C * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(q_target, desc->q_target, (size_t)nsteps * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(A.loss, 0, 8, s));
+    CK(cudaMemcpyAsync(A.q_prev, &P.diag[0].olf_out_cum, 8, cudaMemcpyDeviceToDevice, s));
+
+    // step counters of the checkpoints (host copies uploaded when restoring)
+    PicardCtrl pc0;
+    CK(cudaMemcpyAsync(&pc0, &P.pctrl[0], sizeof(pc0), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    h->adj_step_host.assign(nsteps + 1, 0);
+    for (int t = 0; t <= nsteps; ++t) h->adj_step_host[t] = pc0.step + t;
+
+    // ---- tape and adjoint buffers
+    if (want_grad) {
+        rc |= mem.get(&A.t_psin, (size_t)S * np);
+        rc |= mem.get(&A.t_thetan, (size_t)S * np);
+        rc |= mem.get(&A.t_ktop, (size_t)S * nc);
+        rc |= mem.get(&A.t_ph, (size_t)S * nc);
+        rc |= mem.get(&A.t_psim, (size_t)S * M * np);
+        rc |= mem.get(&A.t_xm, (size_t)S * M * np);
+        rc |= mem.get(&A.t_hin, (size_t)S * nc);
+        rc |= mem.get(&A.t_hsol, (size_t)S * nc);
+        rc |= mem.get(&A.t_thseed, (size_t)S * 3 * nc);
+        rc |= mem.get(&A.t_iters, (size_t)S);
+        for (double **q : {&A.psibar_next, &A.thbar_next, &A.xbar, &A.psimbar, &A.thmbar, &A.cmbar, &A.psinbar,
+                           &A.thnbar, &A.g_lk, &A.g_al, &A.g_n})
+            rc |= mem.get(q, np);
+        for (double **q : {&A.ktopbar_next, &A.phbar, &A.qtbar, &A.hpbar, &A.phsub_bar, &A.olf_Hbar, &A.olf_hbar})
+            rc |= mem.get(q, nc);
+        if (rc) return DHARA_ERR_NOMEM;
+    }
+
+    // One step of the segment starting at t0, recorded into tape slot sl.
+    // One step of the segment starting at t0, recorded into tape slot sl.  In
+    // the first (forward) sweep the overland step runs and its results are
+    // kept; in the recompute sweep they are restored.
+    auto taped_step = [&](int t0, int sl, bool first_sweep) -> int {
+        const size_t t = (size_t)(t0 + sl);
+        CK(cudaMemcpyAsync(A.t_psin + sl * np, P.psin, np * 8, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(A.t_thetan + sl * np, P.thetan, np * 8, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(A.t_ktop + sl * nc, P.ktop, nc * 8, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(A.t_ph + sl * nc, P.ph, nc * 8, cudaMemcpyDeviceToDevice, s));
+        int r = enqueue_subsurface(h, &A, sl);
+        if (r) return r;
+        CK(cudaMemcpyAsync(A.t_iters + sl, &P.pctrl[0].iter, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(A.t_hin + sl * nc, P.h, nc * 8, cudaMemcpyDeviceToDevice, s));
+        if (first_sweep) {
+            r = enqueue_overland(h);
+            if (r) return r;
+        } else {
+            CK(cudaMemcpyAsync(P.H, olf_H_all + t * nc, nc * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(P.h, olf_h_all + t * nc, nc * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(P.ph, olf_h_all + t * nc, nc * 8, cudaMemcpyDeviceToDevice, s));
+        }
+        CK(cudaMemcpyAsync(A.t_hsol + sl * nc, P.H, nc * 8, cudaMemcpyDeviceToDevice, s));
+        LAUNCH(KT_ADJOINT, launch_adj_loss(P, A, t0 + sl, sl, s));
+        return DHARA_OK;
+    };
+
+    // ---- forward sweep: checkpoints, the loss, and the tape of the last
+    // segment (the first one reversed, so it needs no recompute)
+    const int t0_last = (nseg - 1) * K;
+    for (int t = 0; t < nsteps; ++t) {
+        if (t % K == 0) {
+            rc = copy_state(h, ckpt[t / K], false, 0);
+            if (rc) return rc;
+        }
+        if (want_grad && t >= t0_last) {
+            rc = taped_step(t0_last, t - t0_last, true);
+        } else {
+            rc = enqueue_subsurface(h);
+            if (!rc) rc = enqueue_overland(h);
+        }
+        if (rc) return rc;
+        if (want_grad) {
+            CK(cudaMemcpyAsync(olf_H_all + (size_t)t * nc, P.H, nc * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(olf_h_all + (size_t)t * nc, P.h, nc * 8, cudaMemcpyDeviceToDevice, s));
+        }
+        LAUNCH(KT_ADJOINT, launch_adj_loss(P, A, t, -1, s));
+    }
+    CK(cudaMemcpyAsync(loss, A.loss, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    rc = check_device_error(h);
+    if (rc || !want_grad) return rc;
+
+    // the final state and diagnostics, restored after the reverse sweep
+    rc = copy_state(h, ckpt[nseg], false, 0);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(final_H, P.H, nc * 8, cudaMemcpyDeviceToDevice, s));
+    DevDiag diag_final;
+    CK(cudaMemcpyAsync(&diag_final, &P.diag[0], sizeof(DevDiag), cudaMemcpyDeviceToHost, s));
+    for (double *q : {A.psibar_next, A.thbar_next, A.g_lk, A.g_al, A.g_n}) CK(cudaMemsetAsync(q, 0, np * 8, s));
+    for (double *q : {A.ktopbar_next, A.phbar}) CK(cudaMemsetAsync(q, 0, nc * 8, s));
+
+    std::vector<int> iters(S);
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+        const int t0 = seg * K, t1 = std::min(t0 + K, nsteps), ns = t1 - t0;
+        if (seg != nseg - 1) {
+            // recompute the segment from its checkpoint, recording the tape
+            rc = copy_state(h, ckpt[seg], true, t0);
+            if (rc) return rc;
+            for (int sl = 0; sl < ns; ++sl) {
+                rc = taped_step(t0, sl, false);
+                if (rc) return rc;
+            }
+        }
+        CK(cudaMemcpyAsync(iters.data(), A.t_iters, ns * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        rc = check_device_error(h);
+        if (rc) return rc;
+        // reverse through the segment
+        for (int sl = ns - 1; sl >= 0; --sl) {
+            const int t = t0 + sl;
+            A.step_in_seg = sl;
+            CK(cudaMemcpyAsync(P.psin, A.t_psin + sl * np, np * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(P.thetan, A.t_thetan + sl * np, np * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(P.ktop, A.t_ktop + sl * nc, nc * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(P.ph, A.t_ph + sl * nc, nc * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(&P.pctrl[0].step, &h->adj_step_host[t], sizeof(int), cudaMemcpyHostToDevice, s));
+            LAUNCH(KT_PROLOGUE, launch_prologue(P, s));
+            // overland
+            CK(cudaMemcpyAsync(P.h, A.t_hin + sl * nc, nc * 8, cudaMemcpyDeviceToDevice, s));
+            LAUNCH(KT_OLF_AUX, launch_overland_setup(P, h->Ctot, s));
+            LAUNCH(KT_ADJOINT, launch_adj_olf_rhs(P, A, t, s));
+            LAUNCH(KT_OLF_SOLVE, launch_overland_solve(P, h->L, h->Ctot, s));
+            LAUNCH(KT_ADJOINT, launch_adj_olf_coef(P, A, t, h->Ctot, s));
+            LAUNCH(KT_ADJOINT, launch_adj_olf_finish(P, A, s));
+            // subsurface
+            const int Mi = iters[sl] < 1 ? 1 : (iters[sl] > M ? M : iters[sl]);
+            LAUNCH(KT_ADJOINT, launch_adj_epilogue(P, A, sl, Mi, s));
+            for (int m = Mi - 1; m >= 0; --m) {
+                CK(cudaMemsetAsync(&P.gctrl->n_active, 0, 2 * sizeof(int), s));
+                LAUNCH(KT_ADJOINT, launch_adj_matrix(P, A, sl, m, m == Mi - 1, h->mixed, s));
+                LAUNCH(KT_KRYLOV, launch_krylov(P, h->L, s));
+                LAUNCH(KT_ADJOINT, launch_adj_picard(P, A, sl, m, s));
+            }
+            LAUNCH(KT_ADJOINT, launch_adj_prologue(P, A, sl, s));
+            std::swap(A.psibar_next, A.psinbar);
+            std::swap(A.thbar_next, A.thnbar);
+        }
+    }
+    LAUNCH(KT_ADJOINT, launch_adj_initial(P, A, s));
+    CK(cudaStreamSynchronize(s));
+    rc = check_device_error(h);
+    if (rc) return rc;
+
+    // gradients to the caller (pitched -> reference layout)
+    const size_t row = (size_t)D.nx * 8, pitch = (size_t)D.nxp * 8;
+    CK(cudaMemcpy2DAsync(grad_logks, row, A.g_lk + D.off3, pitch, row, (size_t)D.ny * D.nz, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpy2DAsync(grad_alpha, row, A.g_al + D.off3, pitch, row, (size_t)D.ny * D.nz, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpy2DAsync(grad_n, row, A.g_n + D.off3, pitch, row, (size_t)D.ny * D.nz, cudaMemcpyDeviceToHost, s));
+    // restore the state after the forward run
+    rc = copy_state(h, ckpt[nseg], true, nsteps);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(P.H, final_H, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(&P.diag[0], &diag_final, sizeof(DevDiag), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return DHARA_OK;
+}

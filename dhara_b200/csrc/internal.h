@@ -208,5 +208,51 @@ cudaError_t launch_eval_fields(const DevPtrs &P, int which, double *out, cudaStr
 cudaError_t launch_overland_setup(const DevPtrs &P, long long ctot, cudaStream_t s);
 cudaError_t launch_overland_solve(const DevPtrs &P, const LaunchCfg &L, long long ctot, cudaStream_t s);
 cudaError_t launch_overland_finish(const DevPtrs &P, long long ctot, cudaStream_t s);
+// Discrete adjoint (adjoint.cu).  Tape of one checkpoint segment, the
+// carried adjoint state and the gradient accumulators; 3D arrays in the
+// pitched layout of the handle, 2D arrays dense.
+struct AdjPtrs {
+    long long np, nc;          // 3D (pitched) and 2D array lengths
+    int maxiter;               // Picard iterations stored per step
+    int step_in_seg;           // slot of the step being reversed
+    // tape, per step slot s: inputs of the step, every Picard iterate, the
+    // overland input depth and solution, the theta misfit seed
+    double *t_psin, *t_thetan;         // [S][np]
+    double *t_ktop, *t_ph;             // [S][nc]
+    double *t_psim, *t_xm;             // [S][maxiter][np]
+    double *t_hin, *t_hsol;            // [S][nc]
+    double *t_thseed;                  // [S][3][nc]
+    int *t_iters;                      // [S]
+    // loss
+    const double *theta_target;        // [nsteps][3][nc]
+    const double *q_target;            // [nsteps]
+    double *qhist;                     // [nsteps]
+    double *q_prev;                    // [1] boundary outflow total before the step
+    double *loss;                      // [1]
+    double w_q;
+    // carried adjoint of the state after the step being reversed
+    double *psibar_next, *thbar_next;  // [np]
+    double *ktopbar_next, *phbar;      // [nc]
+    // per Picard iteration
+    double *xbar, *psimbar, *thmbar, *cmbar;  // [np]
+    // accumulated adjoint of the step's inputs
+    double *psinbar, *thnbar;          // [np]
+    double *qtbar, *hpbar, *phsub_bar; // [nc]
+    double *olf_Hbar, *olf_hbar;       // [nc]
+    // gradients (pitched 3D)
+    double *g_lk, *g_al, *g_n;
+};
+
+cudaError_t launch_adj_loss(const DevPtrs &P, const AdjPtrs &A, int t, int seed_slot, cudaStream_t s);
+cudaError_t launch_adj_olf_rhs(const DevPtrs &P, const AdjPtrs &A, int t, cudaStream_t s);
+cudaError_t launch_adj_olf_coef(const DevPtrs &P, const AdjPtrs &A, int t, long long ctot, cudaStream_t s);
+cudaError_t launch_adj_olf_finish(const DevPtrs &P, const AdjPtrs &A, cudaStream_t s);
+cudaError_t launch_adj_epilogue(const DevPtrs &P, const AdjPtrs &A, int slot, int iters, cudaStream_t s);
+cudaError_t launch_adj_matrix(const DevPtrs &P, const AdjPtrs &A, int slot, int m, int zero_guess, int mixed,
+                              cudaStream_t s);
+cudaError_t launch_adj_picard(const DevPtrs &P, const AdjPtrs &A, int slot, int m, cudaStream_t s);
+cudaError_t launch_adj_prologue(const DevPtrs &P, const AdjPtrs &A, int slot, cudaStream_t s);
+cudaError_t launch_adj_initial(const DevPtrs &P, const AdjPtrs &A, cudaStream_t s);
+
 cudaError_t configure_3d(LaunchCfg &L, int device, int ntiles);
 cudaError_t configure_2d(LaunchCfg &L, int device);

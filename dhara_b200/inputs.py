@@ -131,6 +131,22 @@ def mixed_512x512x40(seed=2, nx=512, ny=512, nz=40, **kw):
     return make_domain(nx, ny, nz, **args)
 
 
+def adjoint_128x128x30(seed=5, nx=128, ny=128, nz=30, **kw):
+    """The calibration domain: 128x128x30 with the 32x32x20 domain's physics
+    (Ks sigma_ln 0.5, rain 10 mm/h for 1 h, water table 0.8 m), dt 60 s x 120
+    steps, FP32 inner solve + FP64 refinement.  The Picard loop runs its full
+    10 iterations every step (tolerance 1e-300): with a convergence test the
+    number of iterations, and so the computed state, jumps when a parameter
+    moves the error across the tolerance, and the loss is not differentiable
+    at the scale of a finite-difference step."""
+    args = dict(seed=seed, ks_sigma_ln=0.5, rain_mm_per_h=10.0, rain_hours=1.0, nsteps=120,
+                picard_rule=_abi.PICARD_PSI_ABSOLUTE, picard_tol=1e-300, picard_maxiter=10,
+                krylov_tol=1e-10, krylov_maxiter=200, precision=_abi.MIXED,
+                theta_update=_abi.THETA_CONSERVATIVE)
+    args.update(kw)
+    return make_domain(nx, ny, nz, **args)
+
+
 def ensemble(ndomains=256, seed=3, lo=(16, 16, 20), hi=(128, 128, 40), nsteps=120, **kw):
     """Independent domains of uneven size drawn uniformly between lo and hi,
     each with its own seed, Ks sigma_ln in [0.5, 1.5], alpha in [1, 5] /m,

@@ -232,7 +232,8 @@ int dhara_get_stream(dhara_handle *h, void **stream);
 
 /* Per-kernel CUDA-event timing (off by default).  kernel: 0 = 3D Krylov solve,
  * 1 = Picard assembly, 2 = Picard check, 3 = step epilogue, 4 = overland solve,
- * 5 = overland set-up/finish, 6 = step prologue. */
+ * 5 = overland set-up/finish, 6 = step prologue, 7 = the adjoint's own kernels
+ * (its linear solves count under 0 and 4). */
 int dhara_set_kernel_timing(dhara_handle *h, int enable);
 int dhara_get_kernel_timing(dhara_handle *h, int kernel, int64_t *launches, double *total_ms);
 int dhara_reset_kernel_timing(dhara_handle *h);
@@ -241,6 +242,43 @@ int dhara_get_launch_count(dhara_handle *h, int64_t *count);
 /* Algorithmic HBM bytes moved by the 3D Krylov kernel so far (the count the
  * roofline figure divides by time), and the inner iterations they cover. */
 int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations);
+
+/* ---- discrete adjoint ------------------------------------------------------
+ * No counterpart in the reference.  Gradient of a soil-moisture / outflow
+ * misfit with respect to per-cell log Ks, alpha (1/m) and n, by the discrete
+ * adjoint of the implicit time steps with checkpointing: the forward run keeps
+ * the state every checkpoint_every steps; the reverse sweep recomputes each
+ * segment from its checkpoint, recording every Picard iterate, and runs the
+ * adjoint kernels backwards through it (each linear solve reversed by a solve
+ * with the same symmetric matrix).
+ *
+ *   L = sum_t sum_{k<3} sum_c (theta_{t,k,c} - theta_target_{t,k,c})^2
+ *     + w_q * sum_t (Q_t - q_target_t)^2
+ *
+ * theta_{t,k,c}: moisture of layer k (k = 0 the top) of column c after step t;
+ * Q_t: the overland flow into the fixed boundary ring during step t (depth in
+ * m summed over columns).  Scope: a single-domain handle; top flux condition,
+ * free-drainage bottom, no-flux sides (no Dirichlet faces); zero ET and
+ * transpiration. */
+typedef struct {
+    int32_t struct_size;         /* sizeof(dhara_adjoint_desc) */
+    int32_t nsteps;              /* time steps of the run (>= 1) */
+    int32_t checkpoint_every;    /* steps per checkpoint segment (>= 1) */
+    int32_t pad;
+    const double *theta_target;  /* host, [nsteps][3][nx*ny] */
+    const double *q_target;      /* host, [nsteps] */
+    double w_q;                  /* weight of the outflow misfit */
+    double reserved[4];
+} dhara_adjoint_desc;
+
+/* Runs desc->nsteps steps forward from the handle's current state (the state
+ * advances exactly as with dhara_step) and returns the loss in *loss.  When
+ * grad_logks, grad_alpha and grad_n are all non-NULL it also runs the reverse
+ * sweep and writes dL/dlog(Ks), dL/dalpha and dL/dn per cell in the reference
+ * 3D layout (nx*ny*nz values each); when they are all NULL only the loss is
+ * computed. */
+int dhara_adjoint(dhara_handle *h, const dhara_adjoint_desc *desc, double *loss, double *grad_logks,
+                  double *grad_alpha, double *grad_n);
 
 /* ---- allocation-free overland step ---------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
