@@ -341,6 +341,8 @@ __global__ void __launch_bounds__(TILE_THREADS) k_adj_matrix(DevPtrs P, AdjPtrs 
             vg_eval<float>(psi, a, n, D.theta_s, D.theta_r, P.ksat[g], th, Kf, Cf);
             Kv = Kf;
             Cv = Cf;
+        } else if (D.closure_fast) {
+            vg_eval_fast(psi, a, n, D.theta_s, D.theta_r, P.ksat[g], th, Kv, Cv);
         } else {
             vg_eval<double>(psi, a, n, D.theta_s, D.theta_r, P.ksat[g], th, Kv, Cv);
         }

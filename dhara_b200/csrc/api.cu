@@ -454,6 +454,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         D.inner_tol = h->mixed ? (p.inner_tol > 0 ? p.inner_tol : 1e-4) : 0.0;
         D.overland_tol = p.overland_tol;
         D.closure_fp32 = (h->mixed && p.closure_fp32) ? 1 : 0;
+        D.closure_fast = (h->mixed && !p.closure_fp32) ? 1 : 0;
         D.tile_begin = (int)h->htiles.size();
         for (int y0 = 0; y0 < p.ny; y0 += TILE_Y)
             for (int x0 = 0; x0 < p.nx; x0 += TILE_X) h->htiles.push_back({d, x0, y0, 0});

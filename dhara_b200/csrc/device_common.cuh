@@ -224,6 +224,37 @@ __device__ __forceinline__ void vg_eval<double>(double psi, double alpha_m, doub
         C = 0.0;
 }
 
+// The same closure in FP64 arithmetic from fewer transcendental calls: with
+// x = alpha |psi|, u = 1 + x^n and m = 1 - 1/n,
+//   Se = u^-m,  theta = tr + (ts - tr) Se,
+//   (1 - Se^(1/m))^m = (x^n / u)^m,  K = Ks Se^(1/2) (1 - (x^n/u)^m)^2,
+//   C = alpha (n - 1) (ts - tr) x^(n-1) Se / u,
+// from one log, one log1p and three exponentials (expm1 for 1 - (x^n/u)^m).
+// It is more accurate than the reference's expressions where Se is close to
+// 1 (their 1 - Se^(1/m) cancels, leaving ~1e-8 relative noise in K), so it
+// differs from them at that level; the mixed-precision path uses it.
+__device__ __forceinline__ void vg_eval_fast(double psi, double alpha_m, double n, double theta_S,
+                                             double theta_R, double Ksat, double &theta, double &K, double &C) {
+    if (psi < 0.0) {
+        const double x = alpha_m * (-psi);
+        const double lx = log(x);
+        const double xn1 = exp((n - 1.0) * lx);
+        const double xn = xn1 * x;
+        const double m = (n - 1.0) / n;
+        const double lu = log1p(xn);
+        const double Se = exp(-m * lu);
+        theta = theta_R + (theta_S - theta_R) * Se;
+        const double lq = (xn > 1.0) ? -log1p(1.0 / xn) : n * lx - lu;  // log(x^n / u)
+        const double f = -expm1(m * lq);
+        K = Ksat * sqrt(Se) * f * f;
+        C = alpha_m * (n - 1.0) * (theta_S - theta_R) * xn1 * Se / (1.0 + xn);
+    } else {
+        theta = theta_S;
+        K = Ksat;
+        C = 0.0;
+    }
+}
+
 template <>
 __device__ __forceinline__ void vg_eval<float>(double psi_d, double alpha_d, double n_d, double ts,
                                                double tr, double ks, double &theta, float &K, float &C) {

@@ -43,6 +43,7 @@ struct DomainDesc {
     int has_n, picard_rule, theta_update, picard_maxiter;
     int krylov_maxiter, inner_maxiter, overland_maxiter, sched_len;
     int tile_begin, tile_end, closure_fp32, nxp;  // nxp: row pitch of 3D arrays (nx rounded up to 4)
+    int closure_fast, pad_dd;                     // reformulated FP64 closure (mixed mode)
     long long off3, off2, offWE, offSN, sched_off;
     double dx, dy, dz, dt;
     double alpha, n, theta_s, theta_r, porosity, Ss, am;

@@ -24,8 +24,9 @@
 
 #define MAX_CYCLES 30
 
-// The closure of the assembled system: FP64 (the reference's expressions)
-// unless the domain asks for the FP32 closure.
+// The closure of the assembled system: the reference's FP64 expressions in
+// FP64 mode, the reformulated FP64 closure in mixed mode, or the FP32 closure
+// when the domain asks for it.
 __device__ __forceinline__ void closure(const DomainDesc &D, double psi, double a, double n, double ks,
                                         double &th, double &K, double &C) {
     if (D.closure_fp32) {
@@ -33,6 +34,8 @@ __device__ __forceinline__ void closure(const DomainDesc &D, double psi, double 
         vg_eval<float>(psi, a, n, D.theta_s, D.theta_r, ks, th, Kf, Cf);
         K = (double)Kf;
         C = (double)Cf;
+    } else if (D.closure_fast) {
+        vg_eval_fast(psi, a, n, D.theta_s, D.theta_r, ks, th, K, C);
     } else {
         vg_eval<double>(psi, a, n, D.theta_s, D.theta_r, ks, th, K, C);
     }
@@ -935,7 +938,7 @@ __global__ void k_eval_fields(DevPtrs P, int which, double *out) {
         const double a = D.has_alpha ? P.alpha[g] : D.alpha;
         const double n = D.has_n ? P.nvg[g] : D.n;
         double th, Kv, C;
-        vg_eval<double>(P.psin[g], a, n, D.theta_s, D.theta_r, P.ksat[g], th, Kv, C);
+        closure(D, P.psin[g], a, n, P.ksat[g], th, Kv, C);
         out[g] = which == 0 ? th : (which == 1 ? Kv : C);
     }
 }
