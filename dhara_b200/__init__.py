@@ -67,6 +67,10 @@ def lib():
         "dhara_get_launch_count": (ct.c_int, [vp, i64p]),
         "dhara_get_krylov_traffic": (ct.c_int, [vp, dp, i64p]),
         "dhara_adjoint": (ct.c_int, [vp, P(_abi.AdjointDesc), dp, dp, dp, dp]),
+        "dhara_get_params": (ct.c_int, [vp, ct.c_int, P(Params)]),
+        "dhara_params_from_config": (ct.c_int, [ct.c_char_p, ct.c_int, ct.c_int, ct.c_int, P(Params),
+                                                P(_abi.ConfigBC)]),
+        "dhara_apply_boundary_config": (ct.c_int, [vp, ct.c_int, P(_abi.ConfigBC)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -89,6 +93,19 @@ def default_params(nx, ny, nz, dx, dy, dz, dt):
 
 def _dp(a):
     return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+FACES = ("top", "bottom", "north", "south", "east", "west")
+
+
+def params_from_config(path, nx, ny, nz):
+    """The reference's configuration file (src/io.cc:236-274, src/host.cc:93-112)
+    as dhara_params plus per-face boundary settings {face: (type, psi, flux)}."""
+    p = Params()
+    bc = _abi.ConfigBC()
+    _check(lib().dhara_params_from_config(os.fsencode(path), nx, ny, nz, ct.byref(p), ct.byref(bc)))
+    faces = {f: (bc.type[i], bc.psi[i], bc.flux[i]) for i, f in enumerate(FACES)}
+    return p, faces, bc
 
 
 class Solver:
@@ -144,6 +161,10 @@ class Solver:
             self.upload(k, v, domain)
         if schedule and len(dom.rain_mm):
             self.set_rain_schedule(dom.rain_mm, domain)
+
+    def apply_boundary_config(self, bc, domain=0):
+        """Uploads the per-face settings of params_from_config's third result."""
+        _check(lib().dhara_apply_boundary_config(self.h, domain, ct.byref(bc)))
 
     def set_roots(self, rda, nproc, domain=0):
         a = np.ascontiguousarray(rda, np.float64)

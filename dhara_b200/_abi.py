@@ -72,6 +72,12 @@ class Diagnostics(ct.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
+class ConfigBC(ct.Structure):
+    """dhara_config_bc: faces top, bottom, north, south, east, west."""
+    _fields_ = [("type", ct.c_int32 * 6), ("psi", ct.c_double * 6), ("flux", ct.c_double * 6),
+                ("found", ct.c_int32), ("pad", ct.c_int32)]
+
+
 class AdjointDesc(ct.Structure):
     _fields_ = [
         ("struct_size", ct.c_int32), ("nsteps", ct.c_int32), ("checkpoint_every", ct.c_int32),

@@ -380,6 +380,13 @@ __attribute__((visibility("hidden"))) int dhara_internal_fail(int code, const ch
 extern "C" {
 
 const char *dhara_last_error(void) { return g_err.c_str(); }
+
+int dhara_get_params(dhara_handle *h, int domain, dhara_params *out) {
+    if (!h || !out) return fail(DHARA_ERR_INVALID, "NULL argument");
+    if (domain < 0 || domain >= h->ndom) return fail(DHARA_ERR_INVALID, "domain %d out of range", domain);
+    *out = h->params[domain];
+    return DHARA_OK;
+}
 int dhara_abi_version(void) { return DHARA_ABI_VERSION; }
 
 void dhara_default_params(dhara_params *p, int nx, int ny, int nz, double dx, double dy, double dz,

@@ -188,6 +188,9 @@ typedef struct {
 int dhara_create(const dhara_params *params, int ndomains, int device, dhara_handle **out);
 int dhara_destroy(dhara_handle *h);
 
+/* The parameters domain `domain` of the handle was created with. */
+int dhara_get_params(dhara_handle *h, int domain, dhara_params *out);
+
 /* Message of the last failing call on this thread (never NULL). */
 const char *dhara_last_error(void);
 int dhara_abi_version(void);
@@ -242,6 +245,37 @@ int dhara_get_launch_count(dhara_handle *h, int64_t *count);
 /* Algorithmic HBM bytes moved by the 3D Krylov kernel so far (the count the
  * roofline figure divides by time), and the inner iterations they cover. */
 int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations);
+
+/* ---- configuration file ----------------------------------------------------
+ * The reference's "KEY = value" configuration file (parsed by
+ * ParserConfigFile, src/parser.cc:39-72; keys read by LoadFlowModelConfig,
+ * src/io.cc:236-274, and the boundary keys of src/host.cc:93-112).  Lines
+ * starting with '#' are comments; the first occurrence of a key wins; keys
+ * absent from the file keep the value dhara_default_params gives.  Units are
+ * the reference's: ALPHA is read in 1/cm (stored in 1/m), TIME_STEP_DATA is
+ * the model time step in the reference's device time unit (hours) and sets
+ * dt and sec_p_mm2dt_p_m = dt * 3600 / 1000 as include/devconst.h pairs them.
+ * picard_tol is TOLERANCE_PRESSURE for PICARD_METHOD 0 and TOLERANCE_THETA
+ * for PICARD_METHOD 1.  The grid size comes from the caller (the reference
+ * reads it from the topography file). */
+typedef struct {
+    /* faces in the order top, bottom, north, south, east, west */
+    int32_t type[6];     /* BOUNDARY_TYPE_*: 0 Dirichlet, 1 free flow, 2 no flow */
+    double psi[6];       /* PRESSURE_HEAD_* */
+    double flux[6];      /* FLUX_* */
+    int32_t found;       /* number of recognised keys read from the file */
+    int32_t pad;
+} dhara_config_bc;
+
+/* Fills *p (and *bc when not NULL) from the file.  As in the reference
+ * (src/host.cc:101-109), PRESSURE_HEAD_BOTTOM and FLUX_BOTTOM land on the top
+ * face and PRESSURE_HEAD_TOP and FLUX_TOP on the bottom face.  Returns
+ * DHARA_ERR_INVALID if the file cannot be read. */
+int dhara_params_from_config(const char *path, int nx, int ny, int nz, dhara_params *p, dhara_config_bc *bc);
+
+/* Uploads the face types and values of *bc as the boundary arrays of one
+ * domain (constant over each face). */
+int dhara_apply_boundary_config(dhara_handle *h, int domain, const dhara_config_bc *bc);
 
 /* ---- discrete adjoint ------------------------------------------------------
  * No counterpart in the reference.  Gradient of a soil-moisture / outflow
