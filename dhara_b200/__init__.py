@@ -68,6 +68,10 @@ def lib():
         "dhara_get_krylov_traffic": (ct.c_int, [vp, dp, i64p]),
         "dhara_adjoint": (ct.c_int, [vp, P(_abi.AdjointDesc), dp, dp, dp, dp]),
         "dhara_get_params": (ct.c_int, [vp, ct.c_int, P(Params)]),
+        "dhara_enable_statistics": (ct.c_int, [vp, ct.c_int]),
+        "dhara_get_statistics": (ct.c_int, [vp, ct.c_int, i64p, dp, dp, dp]),
+        "dhara_snapshot": (ct.c_int, [vp, ct.c_int, dp, dp, dp, dp]),
+        "dhara_snapshot_wait": (ct.c_int, [vp]),
         "dhara_params_from_config": (ct.c_int, [ct.c_char_p, ct.c_int, ct.c_int, ct.c_int, P(Params),
                                                 P(_abi.ConfigBC)]),
         "dhara_apply_boundary_config": (ct.c_int, [vp, ct.c_int, P(_abi.ConfigBC)]),
@@ -161,6 +165,34 @@ class Solver:
             self.upload(k, v, domain)
         if schedule and len(dom.rain_mm):
             self.set_rain_schedule(dom.rain_mm, domain)
+
+    def enable_statistics(self, max_steps):
+        _check(lib().dhara_enable_statistics(self.h, int(max_steps)))
+
+    def statistics(self, domain=0, max_steps=100000):
+        """Per-step mb_subsurfaceW and layer sums of the head and moisture
+        (the reference's CopyLayers), as arrays [nsteps] and [nsteps, nz]."""
+        nz = self.params[domain].nz
+        n = ct.c_int64()
+        _check(lib().dhara_get_statistics(self.h, domain, ct.byref(n), None, None, None))
+        mb = np.zeros(max(n.value, 1))
+        ps = np.zeros(max(n.value, 1) * nz)
+        th = np.zeros(max(n.value, 1) * nz)
+        _check(lib().dhara_get_statistics(self.h, domain, ct.byref(n), _dp(mb), _dp(ps), _dp(th)))
+        k = n.value
+        return {"mb_subsurfaceW": mb[:k], "pressure_sum": ps[:k * nz].reshape(k, nz),
+                "moisture_sum": th[:k * nz].reshape(k, nz)}
+
+    def snapshot(self, buffers, domain=0):
+        """Queues a copy of the state into the given host arrays (keys
+        water_elevation, water_depth, pressure_head, moisture; pinned for
+        overlap); valid after snapshot_wait()."""
+        ptr = [(_dp(buffers[k]) if k in buffers else None)
+               for k in ("water_elevation", "water_depth", "pressure_head", "moisture")]
+        _check(lib().dhara_snapshot(self.h, domain, *ptr))
+
+    def snapshot_wait(self):
+        _check(lib().dhara_snapshot_wait(self.h))
 
     def apply_boundary_config(self, bc, domain=0):
         """Uploads the per-face settings of params_from_config's third result."""

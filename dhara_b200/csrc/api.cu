@@ -77,6 +77,15 @@ struct dhara_handle {
     long long launches[KT_N] = {};
     long long launch_count = 0;
     std::vector<int> adj_step_host;  // step counters uploaded by the adjoint sweep
+    // per-step statistics (dhara_enable_statistics)
+    int stats_steps = 0;
+    double *stats_part = nullptr, *stats_hist = nullptr;
+    // snapshots (dhara_snapshot): two device staging slots drained by a copy stream
+    cudaStream_t copy_stream = nullptr;
+    double *snap[2] = {nullptr, nullptr};
+    cudaEvent_t snap_ready[2] = {nullptr, nullptr}, snap_done[2] = {nullptr, nullptr};
+    bool snap_used[2] = {false, false};
+    int snap_slot = 0;
 };
 
 namespace {
@@ -204,6 +213,10 @@ int enqueue_subsurface(dhara_handle *h, const AdjPtrs *tape = nullptr, int slot 
         LAUNCH(KT_CHECK, launch_picard_check(P, s));
     }
     LAUNCH(KT_EPILOGUE, launch_epilogue(P, h->L, s));
+    if (h->stats_steps > 0) {
+        LAUNCH(KT_EPILOGUE, launch_layer_stats(P, h->stats_part, h->nz_max, h->stats_hist, h->stats_steps, s));
+        h->launch_count += 1;  // the statistics are two kernels
+    }
     return DHARA_OK;
 }
 
@@ -380,6 +393,108 @@ __attribute__((visibility("hidden"))) int dhara_internal_fail(int code, const ch
 extern "C" {
 
 const char *dhara_last_error(void) { return g_err.c_str(); }
+
+int dhara_enable_statistics(dhara_handle *h, int max_steps) {
+    if (!h || max_steps < 1) return fail(DHARA_ERR_INVALID, "need a handle and max_steps >= 1");
+    if (h->stats_steps > 0) return fail(DHARA_ERR_STATE, "statistics are already enabled");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->stream));
+    const size_t row = 1 + 2 * (size_t)h->nz_max;
+    if (dalloc(h, &h->stats_part, (size_t)h->P.ntiles * h->nz_max * 2)) return DHARA_ERR_NOMEM;
+    if (dalloc(h, &h->stats_hist, (size_t)h->ndom * max_steps * row)) return DHARA_ERR_NOMEM;
+    CK(cudaMemsetAsync(h->stats_hist, 0, (size_t)h->ndom * max_steps * row * 8, h->stream));
+    h->stats_steps = max_steps;
+    if (h->graph_exec) {  // the step sequence changed
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    return DHARA_OK;
+}
+
+int dhara_get_statistics(dhara_handle *h, int domain, int64_t *nsteps, double *mb_subsurfaceW,
+                         double *pressure_sum, double *moisture_sum) {
+    if (!h || !nsteps) return fail(DHARA_ERR_INVALID, "NULL argument");
+    if (domain < 0 || domain >= h->ndom) return fail(DHARA_ERR_INVALID, "domain %d out of range", domain);
+    if (h->stats_steps < 1) return fail(DHARA_ERR_STATE, "statistics are not enabled");
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    PicardCtrl pc;
+    CK(cudaMemcpyAsync(&pc, &h->P.pctrl[domain], sizeof(pc), cudaMemcpyDeviceToHost, h->stream));
+    const size_t row = 1 + 2 * (size_t)h->nz_max;
+    std::vector<double> hist((size_t)h->stats_steps * row);
+    CK(cudaMemcpyAsync(hist.data(), h->stats_hist + (size_t)domain * h->stats_steps * row, hist.size() * 8,
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int n = std::min(pc.step, h->stats_steps);
+    const int nz = h->hdom[domain].nz;
+    *nsteps = n;
+    for (int t = 0; t < n; ++t) {
+        const double *r = hist.data() + (size_t)t * row;
+        if (mb_subsurfaceW) mb_subsurfaceW[t] = r[0];
+        for (int k = 0; k < nz; ++k) {
+            if (pressure_sum) pressure_sum[(size_t)t * nz + k] = r[1 + k];
+            if (moisture_sum) moisture_sum[(size_t)t * nz + k] = r[1 + h->nz_max + k];
+        }
+    }
+    return DHARA_OK;
+}
+
+int dhara_snapshot(dhara_handle *h, int domain, double *water_elevation, double *water_depth,
+                   double *pressure_head, double *moisture) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (domain < 0 || domain >= h->ndom) return fail(DHARA_ERR_INVALID, "domain %d out of range", domain);
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    const DomainDesc &D = h->hdom[domain];
+    const size_t np = (size_t)D.nxp * D.ny * D.nz, nc = (size_t)D.nx * D.ny;
+    const size_t slot_len = 2 * np + 2 * nc;
+    if (!h->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            CK(cudaEventCreateWithFlags(&h->snap_ready[k], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&h->snap_done[k], cudaEventDisableTiming));
+        }
+    }
+    // staging slots sized for the largest domain of the handle
+    if (!h->snap[0]) {
+        size_t most = 0;
+        for (const DomainDesc &E : h->hdom)
+            most = std::max(most, 2 * (size_t)E.nxp * E.ny * E.nz + 2 * (size_t)E.nx * E.ny);
+        for (int k = 0; k < 2; ++k)
+            if (dalloc(h, &h->snap[k], most)) return DHARA_ERR_NOMEM;
+    }
+    (void)slot_len;
+    const int k = h->snap_slot;
+    h->snap_slot ^= 1;
+    double *st = h->snap[k];
+    const DevPtrs &P = h->P;
+    cudaStream_t s = h->stream;
+    // the slot's previous copy-out must be finished before it is overwritten
+    if (h->snap_used[k]) CK(cudaStreamWaitEvent(s, h->snap_done[k], 0));
+    CK(cudaMemcpyAsync(st, P.psin + D.off3, np * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(st + np, P.thetan + D.off3, np * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(st + 2 * np, P.H + D.off2, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(st + 2 * np + nc, P.h + D.off2, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaEventRecord(h->snap_ready[k], s));
+    cudaStream_t c = h->copy_stream;
+    CK(cudaStreamWaitEvent(c, h->snap_ready[k], 0));
+    const size_t row = (size_t)D.nx * 8, pitch = (size_t)D.nxp * 8;
+    if (pressure_head)
+        CK(cudaMemcpy2DAsync(pressure_head, row, st, pitch, row, (size_t)D.ny * D.nz, cudaMemcpyDeviceToHost, c));
+    if (moisture)
+        CK(cudaMemcpy2DAsync(moisture, row, st + np, pitch, row, (size_t)D.ny * D.nz, cudaMemcpyDeviceToHost, c));
+    if (water_elevation) CK(cudaMemcpyAsync(water_elevation, st + 2 * np, nc * 8, cudaMemcpyDeviceToHost, c));
+    if (water_depth) CK(cudaMemcpyAsync(water_depth, st + 2 * np + nc, nc * 8, cudaMemcpyDeviceToHost, c));
+    CK(cudaEventRecord(h->snap_done[k], c));
+    h->snap_used[k] = true;
+    return DHARA_OK;
+}
+
+int dhara_snapshot_wait(dhara_handle *h) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (!h->copy_stream) return DHARA_OK;
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->copy_stream));
+    return DHARA_OK;
+}
 
 int dhara_get_params(dhara_handle *h, int domain, dhara_params *out) {
     if (!h || !out) return fail(DHARA_ERR_INVALID, "NULL argument");
@@ -611,6 +726,12 @@ int dhara_destroy(dhara_handle *h) {
             cudaEventDestroy(pr.second);
         }
     for (cudaEvent_t ev : h->event_pool) cudaEventDestroy(ev);
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+    for (int k = 0; k < 2; ++k) {
+        if (h->snap_ready[k]) cudaEventDestroy(h->snap_ready[k]);
+        if (h->snap_done[k]) cudaEventDestroy(h->snap_done[k]);
+    }
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     for (void *q : h->allocs) cudaFree(q);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -874,7 +995,7 @@ int dhara_step(dhara_handle *h, int nsteps, int use_graph) {
     for (int s = 0; s < nsteps; ++s) {
         if (use_graph && h->graph_exec && !h->timing) {
             CK(cudaGraphLaunch(h->graph_exec, h->stream));
-            h->launch_count += 4 + 3 * (long long)h->maxiter_picard + 3;
+            h->launch_count += 4 + 3 * (long long)h->maxiter_picard + 3 + (h->stats_steps > 0 ? 2 : 0);
         } else {
             int rc = enqueue_subsurface(h);
             if (rc) return rc;

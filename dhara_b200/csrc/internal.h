@@ -255,5 +255,8 @@ cudaError_t launch_adj_picard(const DevPtrs &P, const AdjPtrs &A, int slot, int 
 cudaError_t launch_adj_prologue(const DevPtrs &P, const AdjPtrs &A, int slot, cudaStream_t s);
 cudaError_t launch_adj_initial(const DevPtrs &P, const AdjPtrs &A, cudaStream_t s);
 
+cudaError_t launch_layer_stats(const DevPtrs &P, double *part, int nz_max, double *hist, int max_steps,
+                               cudaStream_t s);
+
 cudaError_t configure_3d(LaunchCfg &L, int device, int ntiles);
 cudaError_t configure_2d(LaunchCfg &L, int device);

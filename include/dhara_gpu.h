@@ -246,6 +246,34 @@ int dhara_get_launch_count(dhara_handle *h, int64_t *count);
  * roofline figure divides by time), and the inner iterations they cover. */
 int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations);
 
+/* ---- output ----------------------------------------------------------------
+ * The reference's outputs (SaveModelResults, src/io.cc:854-915, and
+ * SaveResultEntirePeriod, src/io.cc:962-996) without its blocking per-step
+ * copies (src/subsurface.cu:842-846).
+ *
+ * Statistics: after every step the layer sums of the new head and of
+ * theta(new head) over all cells of the layer but its last (the reference's
+ * CopyLayers range, src/device.cu:135-147; written as pressure_mean and
+ * moisture_mean) and the step's water balance (mb_subsurfaceW) are kept on
+ * the device for up to max_steps steps per domain (counted by the domain's
+ * step counter).  dhara_get_statistics copies them out: mb_subsurfaceW[t],
+ * pressure_sum[t*nz + k], moisture_sum[t*nz + k] for t < *nsteps; any output
+ * pointer may be NULL. */
+int dhara_enable_statistics(dhara_handle *h, int max_steps);
+int dhara_get_statistics(dhara_handle *h, int domain, int64_t *nsteps, double *mb_subsurfaceW,
+                         double *pressure_sum, double *moisture_sum);
+
+/* Snapshot of one domain's state (water_elevation, water_depth: nx*ny;
+ * pressure_head, moisture: nx*ny*nz in the reference layout; any may be NULL):
+ * queued on the handle's stream as a device copy into one of two staging
+ * slots, then copied to the host buffers on a second stream, so the steps
+ * queued after it run while the copy drains (pin the host buffers for that
+ * overlap).  The buffers hold the snapshot once dhara_snapshot_wait returns;
+ * with two sets of buffers a caller can snapshot every step. */
+int dhara_snapshot(dhara_handle *h, int domain, double *water_elevation, double *water_depth,
+                   double *pressure_head, double *moisture);
+int dhara_snapshot_wait(dhara_handle *h);
+
 /* ---- configuration file ----------------------------------------------------
  * The reference's "KEY = value" configuration file (parsed by
  * ParserConfigFile, src/parser.cc:39-72; keys read by LoadFlowModelConfig,

@@ -35,6 +35,7 @@ ALPHA                   = 0.5
 BOUNDARY_TYPE_TOP       = 1
 BOUNDARY_TYPE_BOTTOM    = 0
 BOUNDARY_TYPE_NORTH     = 2
+BOUNDARY_TYPE_WEST      = 0
 PRESSURE_HEAD_TOP       = -0.7
 PRESSURE_HEAD_BOTTOM    = -1.5
 FLUX_TOP                = 1e-6
@@ -68,7 +69,8 @@ def test_boundary_keys_follow_the_reference(cfg):
     assert faces["top"] == (1, -1.5, 2e-6)        # *_BOTTOM values land on the top face
     assert faces["bottom"] == (0, -0.7, 1e-6)     # *_TOP values land on the bottom face
     assert faces["north"][0] == 2 and faces["east"] == (1, 0.0, 3e-7)
-    assert faces["west"] == (1, 0.0, 0.0)         # missing: free flow, zero values
+    assert faces["west"] == (0, 0.0, 0.0)
+    assert faces["south"] == (1, 0.0, 0.0)        # missing: free flow, zero values
 
 
 def test_missing_keys_keep_defaults(tmp_path):
