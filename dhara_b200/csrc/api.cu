@@ -77,6 +77,8 @@ struct dhara_handle {
     long long launches[KT_N] = {};
     long long launch_count = 0;
     std::vector<int> adj_step_host;  // step counters uploaded by the adjoint sweep
+    bool any_dirichlet = false;      // some domain has a type-0 face
+    std::vector<std::vector<bool>> face_dirichlet;  // [domain][W, E, S, N, B]
     // per-step statistics (dhara_enable_statistics)
     int stats_steps = 0;
     double *stats_part = nullptr, *stats_hist = nullptr;
@@ -204,6 +206,10 @@ int enqueue_subsurface(dhara_handle *h, const AdjPtrs *tape = nullptr, int slot 
     LAUNCH(KT_PROLOGUE, launch_prologue(P, s));
     for (int m = 0; m < h->maxiter_picard; ++m) {
         LAUNCH(KT_ASSEMBLE, launch_assemble(P, h->L, s));
+        if (h->any_dirichlet) {
+            LAUNCH(KT_ASSEMBLE, launch_dirichlet(P, h->L, s));
+            h->launch_count += 1;  // two kernels
+        }
         LAUNCH(KT_KRYLOV, launch_krylov(P, h->L, s));
         if (tape) {
             const size_t off = ((size_t)slot * tape->maxiter + m) * tape->np;
@@ -283,9 +289,11 @@ int locate(dhara_handle *h, int dom, int field, FieldLoc *out) {
         case DHARA_F_BCQE: f.ptr = P.bcqe + D.offWE; f.count = WE; break;
         case DHARA_F_BCQS: f.ptr = P.bcqs + D.offSN; f.count = SN; break;
         case DHARA_F_BCQN: f.ptr = P.bcqn + D.offSN; f.count = SN; break;
-        case DHARA_F_BCPSIW: case DHARA_F_BCPSIE: f.count = WE; break;
-        case DHARA_F_BCPSIS: case DHARA_F_BCPSIN: f.count = SN; break;
-        case DHARA_F_BCPSIB: f.count = C; break;
+        case DHARA_F_BCPSIW: f.ptr = P.psi_w + D.offWE; f.count = WE; break;
+        case DHARA_F_BCPSIE: f.ptr = P.psi_e + D.offWE; f.count = WE; break;
+        case DHARA_F_BCPSIS: f.ptr = P.psi_s + D.offSN; f.count = SN; break;
+        case DHARA_F_BCPSIN: f.ptr = P.psi_n + D.offSN; f.count = SN; break;
+        case DHARA_F_BCPSIB: f.ptr = P.psi_b + D.off2; f.count = C; break;
         case DHARA_FI_BCW: case DHARA_FI_BCE: f.count = WE; f.is_int = true; f.elt = 4; break;
         case DHARA_FI_BCS: case DHARA_FI_BCN: f.count = SN; f.is_int = true; f.elt = 4; break;
         case DHARA_FI_BCB: case DHARA_FI_BCT: f.count = C; f.is_int = true; f.elt = 4; break;
@@ -605,6 +613,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     h->roots.assign(ndomains, std::vector<double>());
     h->sched.assign(ndomains, std::vector<double>());
     h->uploaded.assign(ndomains, 0u);
+    h->face_dirichlet.assign(ndomains, std::vector<bool>(5, false));
 
     DevPtrs &P = h->P;
     const size_t N = (size_t)h->Ntot, C = (size_t)h->Ctot;
@@ -636,6 +645,16 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     rc |= dalloc(h, &P.bcqe, (size_t)h->WEtot);
     rc |= dalloc(h, &P.bcqs, (size_t)h->SNtot);
     rc |= dalloc(h, &P.bcqn, (size_t)h->SNtot);
+    rc |= dalloc(h, &P.psi_w, (size_t)h->WEtot);
+    rc |= dalloc(h, &P.psi_e, (size_t)h->WEtot);
+    rc |= dalloc(h, &P.psi_s, (size_t)h->SNtot);
+    rc |= dalloc(h, &P.psi_n, (size_t)h->SNtot);
+    rc |= dalloc(h, &P.psi_b, C);
+    rc |= dalloc(h, &P.dir_w, (size_t)h->WEtot);
+    rc |= dalloc(h, &P.dir_e, (size_t)h->WEtot);
+    rc |= dalloc(h, &P.dir_s, (size_t)h->SNtot);
+    rc |= dalloc(h, &P.dir_n, (size_t)h->SNtot);
+    rc |= dalloc(h, &P.dir_b, C);
     rc |= dalloc(h, &P.procmap, C);
     P.nproc_max = 1;
     P.rda_stride = h->nz_max;
@@ -682,6 +701,12 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     e = e ? e : zero(P.bcqe, (size_t)h->WEtot * 8);
     e = e ? e : zero(P.bcqs, (size_t)h->SNtot * 8);
     e = e ? e : zero(P.bcqn, (size_t)h->SNtot * 8);
+    for (double *q : {P.psi_w, P.psi_e}) e = e ? e : zero(q, (size_t)h->WEtot * 8);
+    for (double *q : {P.psi_s, P.psi_n}) e = e ? e : zero(q, (size_t)h->SNtot * 8);
+    e = e ? e : zero(P.psi_b, C * 8);
+    for (unsigned char *q : {P.dir_w, P.dir_e}) e = e ? e : zero(q, (size_t)h->WEtot);
+    for (unsigned char *q : {P.dir_s, P.dir_n}) e = e ? e : zero(q, (size_t)h->SNtot);
+    e = e ? e : zero(P.dir_b, C);
     e = e ? e : zero(P.procmap, C * 4);
     e = e ? e : zero(P.rda, (size_t)ndomains * P.rda_stride * 8);
     e = e ? e : zero(P.kctrl, ndomains * sizeof(KrylovCtrl));
@@ -792,10 +817,39 @@ int dhara_upload_int(dhara_handle *h, int domain, int field, const int32_t *src,
         return DHARA_OK;
     }
     if (field == DHARA_FI_BCT) return DHARA_OK;  // the top is always a flux face (src/global.cu:236-251)
-    for (int64_t i = 0; i < count; ++i)
-        if (src[i] == 0)
-            return fail(DHARA_ERR_UNSUPPORTED,
-                        "Dirichlet (type 0) side/bottom faces are not implemented on the GPU path");
+    // side and bottom faces: 1 where the face is Dirichlet (type 0)
+    DevPtrs &P = h->P;
+    DomainDesc &D = h->hdom[domain];
+    unsigned char *dst = nullptr;
+    switch (field) {
+        case DHARA_FI_BCW: dst = P.dir_w + D.offWE; break;
+        case DHARA_FI_BCE: dst = P.dir_e + D.offWE; break;
+        case DHARA_FI_BCS: dst = P.dir_s + D.offSN; break;
+        case DHARA_FI_BCN: dst = P.dir_n + D.offSN; break;
+        case DHARA_FI_BCB: dst = P.dir_b + D.off2; break;
+        default: return fail(DHARA_ERR_INVALID, "field %d is not a boundary type field", field);
+    }
+    std::vector<unsigned char> flags((size_t)count);
+    bool any = false;
+    for (int64_t i = 0; i < count; ++i) {
+        flags[(size_t)i] = src[i] == 0 ? 1 : 0;
+        any = any || src[i] == 0;
+    }
+    CK(cudaMemcpyAsync(dst, flags.data(), (size_t)count, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->face_dirichlet[domain][field - DHARA_FI_BCW] = any;
+    bool dom_any = false;
+    for (bool b : h->face_dirichlet[domain]) dom_any = dom_any || b;
+    if ((D.has_dirichlet != 0) != dom_any) {
+        D.has_dirichlet = dom_any ? 1 : 0;
+        if (upload_dom_desc(h)) return DHARA_ERR_CUDA;
+    }
+    h->any_dirichlet = false;
+    for (const DomainDesc &E : h->hdom) h->any_dirichlet = h->any_dirichlet || E.has_dirichlet;
+    if (h->graph_exec) {  // the step sequence may change
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
     return DHARA_OK;
 }
 
@@ -995,7 +1049,8 @@ int dhara_step(dhara_handle *h, int nsteps, int use_graph) {
     for (int s = 0; s < nsteps; ++s) {
         if (use_graph && h->graph_exec && !h->timing) {
             CK(cudaGraphLaunch(h->graph_exec, h->stream));
-            h->launch_count += 4 + 3 * (long long)h->maxiter_picard + 3 + (h->stats_steps > 0 ? 2 : 0);
+            h->launch_count += 4 + 3 * (long long)h->maxiter_picard + 3 + (h->stats_steps > 0 ? 2 : 0) +
+                               (h->any_dirichlet ? 2 * (long long)h->maxiter_picard : 0);
         } else {
             int rc = enqueue_subsurface(h);
             if (rc) return rc;
@@ -1181,6 +1236,7 @@ int dhara_adjoint(dhara_handle *h, const dhara_adjoint_desc *desc, double *loss,
         return fail(DHARA_ERR_INVALID, "struct_size %d != sizeof(dhara_adjoint_desc) %d", desc->struct_size,
                     (int)sizeof(dhara_adjoint_desc));
     if (h->ndom != 1) return fail(DHARA_ERR_UNSUPPORTED, "the adjoint runs on single-domain handles");
+    if (h->any_dirichlet) return fail(DHARA_ERR_UNSUPPORTED, "the adjoint does not cover Dirichlet faces");
     if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
     if (desc->nsteps < 1 || desc->checkpoint_every < 1 || !desc->theta_target || !desc->q_target)
         return fail(DHARA_ERR_INVALID, "adjoint: need nsteps >= 1, checkpoint_every >= 1 and both targets");

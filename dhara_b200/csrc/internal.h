@@ -43,7 +43,7 @@ struct DomainDesc {
     int has_n, picard_rule, theta_update, picard_maxiter;
     int krylov_maxiter, inner_maxiter, overland_maxiter, sched_len;
     int tile_begin, tile_end, closure_fp32, nxp;  // nxp: row pitch of 3D arrays (nx rounded up to 4)
-    int closure_fast, pad_dd;                     // reformulated FP64 closure (mixed mode)
+    int closure_fast, has_dirichlet;              // reformulated FP64 closure (mixed mode); any type-0 face
     long long off3, off2, offWE, offSN, sched_off;
     double dx, dy, dz, dt;
     double alpha, n, theta_s, theta_r, porosity, Ss, am;
@@ -170,6 +170,9 @@ struct DevPtrs {
     int nseg, pad_seg;
     // faces
     double *bcqw, *bcqe, *bcqs, *bcqn;
+    // Dirichlet faces: 1 where the face is type 0, and the fixed heads
+    unsigned char *dir_w, *dir_e, *dir_s, *dir_n, *dir_b;
+    double *psi_w, *psi_e, *psi_s, *psi_n, *psi_b;
     int *procmap;
     double *rda;         // [ndom][nproc_max*nz_max]
     int nproc_max, rda_stride;
@@ -203,6 +206,7 @@ cudaError_t launch_prepare(const DevPtrs &P, int mixed, cudaStream_t s);
 cudaError_t launch_prologue(const DevPtrs &P, cudaStream_t s);
 cudaError_t launch_assemble(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
 cudaError_t launch_krylov(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
+cudaError_t launch_dirichlet(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
 cudaError_t launch_picard_check(const DevPtrs &P, cudaStream_t s);
 cudaError_t launch_epilogue(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
 cudaError_t launch_eval_fields(const DevPtrs &P, int which, double *out, cudaStream_t s);

@@ -203,17 +203,20 @@ __global__ void __launch_bounds__(TILE_THREADS) k_assemble(DevPtrs P) {
                      (P.thetan[g] - thm) / dt + trodz / dt;
         const double dz2inv = -1.0 / (dz * dz), dy2inv = -1.0 / (dy * dy), dx2inv = -1.0 / (dx * dx);
         if (k == 0) rhs += (-P.qtop[cr.c] * dz) * dz2inv;
-        if (k == nz - 1) {
+        const long long bi = D.offWE + (long long)k * cr.ny + cr.j;
+        const long long bj = D.offSN + (long long)k * cr.nx + cr.i;
+        // Neumann terms only on non-Dirichlet faces (a Dirichlet face's rows are
+        // set by k_dir_fixed / k_dir_rows after this kernel)
+        const bool dd = D.has_dirichlet != 0;
+        if (k == nz - 1 && !(dd && P.dir_b[cr.c])) {
             const double qb = K_c;
             P.bcqb[cr.c] = qb;
             rhs += (qb * dz) * dz2inv;
         }
-        const long long bi = D.offWE + (long long)k * cr.ny + cr.j;
-        const long long bj = D.offSN + (long long)k * cr.nx + cr.i;
-        if (cr.j == 0) rhs += (-P.bcqs[bj] * dy) * dy2inv;
-        if (cr.j == cr.ny - 1) rhs += (P.bcqn[bj] * dy) * dy2inv;
-        if (cr.i == 0) rhs += (-P.bcqw[bi] * dx) * dx2inv;
-        if (cr.i == cr.nx - 1) rhs += (P.bcqe[bi] * dx) * dx2inv;
+        if (cr.j == 0 && !(dd && P.dir_s[bj])) rhs += (-P.bcqs[bj] * dy) * dy2inv;
+        if (cr.j == cr.ny - 1 && !(dd && P.dir_n[bj])) rhs += (P.bcqn[bj] * dy) * dy2inv;
+        if (cr.i == 0 && !(dd && P.dir_w[bi])) rhs += (-P.bcqw[bi] * dx) * dx2inv;
+        if (cr.i == cr.nx - 1 && !(dd && P.dir_e[bi])) rhs += (P.bcqe[bi] * dx) * dx2inv;
 
         const double Dv = ssc * thm + Cm / dt;
         P.psim[g] = psi_c;
@@ -230,6 +233,138 @@ __global__ void __launch_bounds__(TILE_THREADS) k_assemble(DevPtrs P) {
         th_c = th_n;
         K_c = K_n;
         C_c = C_n;
+    }
+}
+
+// ---------------------------------------------------------- Dirichlet faces
+// The reference turns each Dirichlet (type 0) face into identity rows for the
+// boundary cells and eliminates their coupling from the next row in, walking
+// the faces in the order top, bottom, south, north, west, east
+// (SetUpBoundaryConditionsSubsurface, src/subsurface.cu:126-353).  Two of its
+// details are kept: the rows next to a west/east/south/north face move the
+// fixed head to the right-hand side with the conductance of the face on the
+// other side of the row (ke for a west face, kw for east, kn for south, ks for
+// north), and a row already set to the identity by an earlier face still takes
+// the right-hand-side terms of later faces.  Here the identity rows are cells
+// whose storage diagonal is set to -1 (the Krylov phases skip them) and whose
+// iterate holds the row's right-hand side; the matrix-free stencil of the next
+// row in couples to that value, so its right-hand side is corrected to the
+// reference's elimination.
+struct DirFaces {
+    bool b, s, n, w, e;
+    double pb, ps, pn, pw, pe;
+};
+
+__device__ __forceinline__ DirFaces dir_faces(const DevPtrs &P, const DomainDesc &D, const ColumnRef &cr, int k) {
+    const long long bi = D.offWE + (long long)k * cr.ny + cr.j;
+    const long long bj = D.offSN + (long long)k * cr.nx + cr.i;
+    DirFaces f;
+    f.b = P.dir_b[cr.c] != 0;
+    f.s = P.dir_s[bj] != 0;
+    f.n = P.dir_n[bj] != 0;
+    f.w = P.dir_w[bi] != 0;
+    f.e = P.dir_e[bi] != 0;
+    f.pb = f.b ? P.psi_b[cr.c] : 0.0;
+    f.ps = f.s ? P.psi_s[bj] : 0.0;
+    f.pn = f.n ? P.psi_n[bj] : 0.0;
+    f.pw = f.w ? P.psi_w[bi] : 0.0;
+    f.pe = f.e ? P.psi_e[bi] : 0.0;
+    return f;
+}
+
+// Face conductances of a cell from K^m (K64), zero on domain faces.
+struct FaceK {
+    double kw, ke, ks, kn, kd, ku;
+};
+__device__ __forceinline__ FaceK face_k(const DevPtrs &P, const ColumnRef &cr, long long g, int k) {
+    const double *K = P.K64;
+    const double Kc = K[g];
+    FaceK f;
+    f.kw = cr.i > 0 ? 0.5 * (Kc + K[g - 1]) : 0.0;
+    f.ke = cr.i < cr.nx - 1 ? 0.5 * (Kc + K[g + 1]) : 0.0;
+    f.ks = cr.j > 0 ? 0.5 * (Kc + K[g - cr.nxp]) : 0.0;
+    f.kn = cr.j < cr.ny - 1 ? 0.5 * (Kc + K[g + cr.nxp]) : 0.0;
+    f.kd = k > 0 ? 0.5 * (Kc + K[g - cr.sxy]) : 0.0;
+    f.ku = k < cr.nz - 1 ? 0.5 * (Kc + K[g + cr.sxy]) : 0.0;
+    return f;
+}
+
+// The reference's right-hand side of a cell after the face rules, starting
+// from the assembled value v; returns whether an identity row was set.
+__device__ __forceinline__ bool dir_rules(const ColumnRef &cr, int k, const DirFaces &f, const FaceK &fk,
+                                          const DomainDesc &D, double &v) {
+    const double ix2 = 1.0 / (D.dx * D.dx), iy2 = 1.0 / (D.dy * D.dy), iz2 = 1.0 / (D.dz * D.dz);
+    bool fixed = false;
+    if (f.b) {
+        if (k == cr.nz - 2) v += iz2 * fk.ku * f.pb;
+        if (k == cr.nz - 1) { v = f.pb; fixed = true; }
+    }
+    if (f.s) {
+        if (cr.j == 1) v += iy2 * fk.kn * f.ps;
+        if (cr.j == 0) { v = f.ps; fixed = true; }
+    }
+    if (f.n) {
+        if (cr.j == cr.ny - 2) v += iy2 * fk.ks * f.pn;
+        if (cr.j == cr.ny - 1) { v = f.pn; fixed = true; }
+    }
+    if (f.w) {
+        if (cr.i == 1) v += ix2 * fk.ke * f.pw;
+        if (cr.i == 0) { v = f.pw; fixed = true; }
+    }
+    if (f.e) {
+        if (cr.i == cr.nx - 2) v += ix2 * fk.kw * f.pe;
+        if (cr.i == cr.nx - 1) { v = f.pe; fixed = true; }
+    }
+    return fixed;
+}
+
+// Pass 1: identity rows (D = -1, x = b = the row's right-hand side).
+template <typename T>
+__global__ void __launch_bounds__(TILE_THREADS) k_dir_fixed(DevPtrs P) {
+    const int tile = blockIdx.x;
+    const TileDesc td = P.tiles[tile];
+    const DomainDesc &D = P.dom[td.dom];
+    if (!D.has_dirichlet || P.pctrl[td.dom].done) return;
+    const ColumnRef cr = column_of(P, tile);
+    if (!cr.valid) return;
+    long long g = cr.g0;
+    for (int k = 0; k < cr.nz; ++k, g += cr.sxy) {
+        const DirFaces f = dir_faces(P, D, cr, k);
+        if (!(f.b || f.s || f.n || f.w || f.e)) continue;
+        double v = P.b[g];
+        if (!dir_rules(cr, k, f, face_k(P, cr, g, k), D, v)) continue;
+        P.b[g] = v;
+        P.x[g] = v;
+        P.D64[g] = -1.0;
+        if (!std::is_same<T, double>::value) ((T *)P.D)[g] = T(-1);
+    }
+}
+
+// Pass 2: the rows next to identity rows get the reference's elimination
+// terms, less the coupling the matrix-free stencil applies to the fixed value.
+template <typename T>
+__global__ void __launch_bounds__(TILE_THREADS) k_dir_rows(DevPtrs P) {
+    const int tile = blockIdx.x;
+    const TileDesc td = P.tiles[tile];
+    const DomainDesc &D = P.dom[td.dom];
+    if (!D.has_dirichlet || P.pctrl[td.dom].done) return;
+    const ColumnRef cr = column_of(P, tile);
+    if (!cr.valid) return;
+    const double ix2 = 1.0 / (D.dx * D.dx), iy2 = 1.0 / (D.dy * D.dy), iz2 = 1.0 / (D.dz * D.dz);
+    long long g = cr.g0;
+    for (int k = 0; k < cr.nz; ++k, g += cr.sxy) {
+        if (P.D64[g] < 0.0) continue;  // identity row
+        const DirFaces f = dir_faces(P, D, cr, k);
+        if (!(f.b || f.s || f.n || f.w || f.e)) continue;
+        const FaceK fk = face_k(P, cr, g, k);
+        double v = P.b[g];
+        dir_rules(cr, k, f, fk, D, v);
+        if (f.b && k == cr.nz - 2) v -= iz2 * fk.ku * P.x[g + cr.sxy];
+        if (f.s && cr.j == 1) v -= iy2 * fk.ks * P.x[g - cr.nxp];
+        if (f.n && cr.j == cr.ny - 2) v -= iy2 * fk.kn * P.x[g + cr.nxp];
+        if (f.w && cr.i == 1) v -= ix2 * fk.kw * P.x[g - 1];
+        if (f.e && cr.i == cr.nx - 2) v -= ix2 * fk.ke * P.x[g + 1];
+        P.b[g] = v;
     }
 }
 
@@ -481,10 +616,13 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
         const double kw = M.w * 0.5 * (Kc + Kw), ke = M.e * 0.5 * (Kc + Ke);
         const double ks = M.s * 0.5 * (Kc + Ks), kn = M.n * 0.5 * (Kc + Kn);
         const double Dk = sD[oc], bk = sb_[oc];
+        // D < 0 marks a Dirichlet (fixed) cell: identity row, x already holds its
+        // value, so its residual is zero and the preconditioner leaves it alone
+        const bool fixed = Dk < 0.0;
         const double Ax = Dk * xc + cx * (kw * (xc - sx[hc - 1]) + ke * (xc - sx[hc + 1])) +
                           cy * (ks * (xc - sx[hc - H::BW]) + kn * (xc - sx[hc + H::BW])) +
                           cz * (kd * (xc - x_up) + ku * (xc - x_dn));
-        const double rk = bk - Ax;
+        const double rk = fixed ? 0.0 : bk - Ax;
         v[0] += rk * rk;
         v[1] += bk * bk;
         const T rT = (T)rk;
@@ -497,14 +635,14 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
         const T bd = (T)Dk + w.cx * (kwT + keT) + w.cy * (ksT + knT) + w.cz * (kdT + kuT);
         const T a = -w.cz * kdT, c = -w.cz * kuT;
         const T den = bd - a * cprev;
-        const T inv = recip(den);
+        const T inv = fixed ? T(0) : recip(den);
         const T cp = c * inv, e = a * inv;
         const T dp = rT * inv - e * dprev;
         finv[g] = inv;
         fe[g] = e;
         fc[g] = cp;
         put_dprime<T, DSMEM>(dp, s_d, k, z + g);
-        v[2] += (double)den * (double)dp * (double)dp;
+        if (!fixed) v[2] += (double)den * (double)dp * (double)dp;
         cprev = cp;
         dprev = dp;
         x_up = xc;
@@ -563,9 +701,11 @@ __device__ void phase_A(const DevPtrs &P, int tile, int tile_next, bool prefetch
         const T kd = mu * (T(0.5) * (Kc + K_up)), ku = md * (T(0.5) * (Kc + K_dn));
         const T kw = mW * (T(0.5) * (Kc + sK[hc - 1])), ke = mE * (T(0.5) * (Kc + sK[hc + 1]));
         const T ks = mS * (T(0.5) * (Kc + sK[hc - H::BW])), kn = mN * (T(0.5) * (Kc + sK[hc + H::BW]));
-        const T Ap = sD[oc] * pc + w.cx * (kw * (pc - pv(sz, sq, hc - 1)) + ke * (pc - pv(sz, sq, hc + 1))) +
-                     w.cy * (ks * (pc - pv(sz, sq, hc - H::BW)) + kn * (pc - pv(sz, sq, hc + H::BW))) +
-                     w.cz * (kd * (pc - p_up) + ku * (pc - p_dn));
+        const T Dk = sD[oc];
+        T Ap = Dk * pc + w.cx * (kw * (pc - pv(sz, sq, hc - 1)) + ke * (pc - pv(sz, sq, hc + 1))) +
+               w.cy * (ks * (pc - pv(sz, sq, hc - H::BW)) + kn * (pc - pv(sz, sq, hc + H::BW))) +
+               w.cz * (kd * (pc - p_up) + ku * (pc - p_dn));
+        if (Dk < T(0)) Ap = T(0);  // Dirichlet cell: p is zero there and its row is the identity
         v[0] += (double)pc * (double)Ap;
         const long long g = cr.g0 + (long long)k * cr.sxy;
         pnew[g] = pc;
@@ -613,7 +753,7 @@ __device__ void phase_B(const DevPtrs &P, int tile, int tile_next, bool prefetch
         v[0] += (double)rk * (double)rk;
         const T dp = rk * inv - e * dprev;
         put_dprime<T, DSMEM>(dp, s_d, k, z + g);
-        v[1] += (double)dp * (double)dp / (double)inv;
+        if (inv != T(0)) v[1] += (double)dp * (double)dp / (double)inv;
         dprev = dp;
     };
     march<CHN, false>(nz, sb, prefetched, issue, plane, issue_next);
@@ -900,7 +1040,10 @@ __global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
             P.K64[g] = K1;
             if (k == 0) P.ktop[cr.c] = K1;
         }
-        const double qt = P.qtop[cr.c], qb = P.bcqb[cr.c];
+        // a Dirichlet bottom has no prescribed flux (the reference keeps q_b out
+        // of its balance there too)
+        const double qt = P.qtop[cr.c];
+        const double qb = (D.has_dirichlet && P.dir_b[cr.c]) ? 0.0 : P.bcqb[cr.c];
         v[3] += (qb - qt) * dt;
         v[5] += qt * dt;
         v[6] += qb * dt;
@@ -980,6 +1123,17 @@ cudaError_t launch_assemble(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s
 cudaError_t launch_epilogue(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s) {
     if (L.mixed) k_epilogue<float><<<P.ntiles, TILE_THREADS, 0, s>>>(P);
     else k_epilogue<double><<<P.ntiles, TILE_THREADS, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dirichlet(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s) {
+    if (L.mixed) {
+        k_dir_fixed<float><<<P.ntiles, TILE_THREADS, 0, s>>>(P);
+        k_dir_rows<float><<<P.ntiles, TILE_THREADS, 0, s>>>(P);
+    } else {
+        k_dir_fixed<double><<<P.ntiles, TILE_THREADS, 0, s>>>(P);
+        k_dir_rows<double><<<P.ntiles, TILE_THREADS, 0, s>>>(P);
+    }
     return cudaGetLastError();
 }
 
