@@ -69,6 +69,9 @@ def lib():
         "dhara_adjoint": (ct.c_int, [vp, P(_abi.AdjointDesc), dp, dp, dp, dp]),
         "dhara_get_params": (ct.c_int, [vp, ct.c_int, P(Params)]),
         "dhara_enable_statistics": (ct.c_int, [vp, ct.c_int]),
+        "dhara_autotune": (ct.c_int, [vp, ct.c_int, P(_abi.LaunchConfig)]),
+        "dhara_get_launch_config": (ct.c_int, [vp, P(_abi.LaunchConfig)]),
+        "dhara_set_launch_config": (ct.c_int, [vp, P(_abi.LaunchConfig)]),
         "dhara_get_statistics": (ct.c_int, [vp, ct.c_int, i64p, dp, dp, dp]),
         "dhara_snapshot": (ct.c_int, [vp, ct.c_int, dp, dp, dp, dp]),
         "dhara_snapshot_wait": (ct.c_int, [vp]),
@@ -165,6 +168,24 @@ class Solver:
             self.upload(k, v, domain)
         if schedule and len(dom.rain_mm):
             self.set_rain_schedule(dom.rain_mm, domain)
+
+    def autotune(self, trial_steps=2):
+        """Times the persistent solvers' block schedules on this handle's data
+        (state restored afterwards) and keeps the fastest."""
+        c = _abi.LaunchConfig()
+        _check(lib().dhara_autotune(self.h, int(trial_steps), ct.byref(c)))
+        return c.as_dict()
+
+    def launch_config(self):
+        c = _abi.LaunchConfig()
+        _check(lib().dhara_get_launch_config(self.h, ct.byref(c)))
+        return c.as_dict()
+
+    def set_launch_config(self, krylov_blocks_per_sm, overland_resident, overland_blocks_per_sm):
+        c = _abi.LaunchConfig()
+        c.krylov_blocks_per_sm, c.overland_resident = krylov_blocks_per_sm, overland_resident
+        c.overland_blocks_per_sm = overland_blocks_per_sm
+        _check(lib().dhara_set_launch_config(self.h, ct.byref(c)))
 
     def enable_statistics(self, max_steps):
         _check(lib().dhara_enable_statistics(self.h, int(max_steps)))

@@ -72,6 +72,15 @@ class Diagnostics(ct.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
+class LaunchConfig(ct.Structure):
+    _fields_ = [("krylov_blocks_per_sm", ct.c_int32), ("overland_resident", ct.c_int32),
+                ("overland_blocks_per_sm", ct.c_int32), ("pad", ct.c_int32),
+                ("krylov_ms", ct.c_double), ("overland_ms", ct.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "pad"}
+
+
 class ConfigBC(ct.Structure):
     """dhara_config_bc: faces top, bottom, north, south, east, west."""
     _fields_ = [("type", ct.c_int32 * 6), ("psi", ct.c_double * 6), ("flux", ct.c_double * 6),

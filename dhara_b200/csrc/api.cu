@@ -1452,3 +1452,175 @@ int dhara_adjoint(dhara_handle *h, const dhara_adjoint_desc *desc, double *loss,
     CK(cudaStreamSynchronize(s));
     return DHARA_OK;
 }
+
+// ---------------------------------------------------------------- autotune
+namespace {
+
+struct SavedState {
+    std::vector<void *> bufs;
+    double *psin = nullptr, *thetan = nullptr, *ktop = nullptr, *ph = nullptr, *hh = nullptr, *H = nullptr;
+    std::vector<PicardCtrl> pctrl;
+    std::vector<DevDiag> diag;
+    ~SavedState() {
+        for (void *p : bufs) cudaFree(p);
+    }
+};
+
+int save_state(dhara_handle *h, SavedState &st) {
+    const size_t np = (size_t)h->Ntot, nc = (size_t)h->Ctot;
+    for (double **q : {&st.psin, &st.thetan}) {
+        if (cudaMalloc((void **)q, np * 8) != cudaSuccess) return fail(DHARA_ERR_NOMEM, "autotune: no memory");
+        st.bufs.push_back(*q);
+    }
+    for (double **q : {&st.ktop, &st.ph, &st.hh, &st.H}) {
+        if (cudaMalloc((void **)q, nc * 8) != cudaSuccess) return fail(DHARA_ERR_NOMEM, "autotune: no memory");
+        st.bufs.push_back(*q);
+    }
+    const DevPtrs &P = h->P;
+    cudaStream_t s = h->stream;
+    CK(cudaMemcpyAsync(st.psin, P.psin, np * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(st.thetan, P.thetan, np * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(st.ktop, P.ktop, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(st.ph, P.ph, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(st.hh, P.h, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(st.H, P.H, nc * 8, cudaMemcpyDeviceToDevice, s));
+    st.pctrl.resize(h->ndom);
+    st.diag.resize(h->ndom);
+    CK(cudaMemcpyAsync(st.pctrl.data(), P.pctrl, h->ndom * sizeof(PicardCtrl), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(st.diag.data(), P.diag, h->ndom * sizeof(DevDiag), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return DHARA_OK;
+}
+
+int restore_state(dhara_handle *h, const SavedState &st) {
+    const size_t np = (size_t)h->Ntot, nc = (size_t)h->Ctot;
+    const DevPtrs &P = h->P;
+    cudaStream_t s = h->stream;
+    CK(cudaMemcpyAsync(P.psin, st.psin, np * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.x, st.psin, np * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.psim, st.psin, np * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.thetan, st.thetan, np * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.ktop, st.ktop, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.ph, st.ph, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.h, st.hh, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.H, st.H, nc * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.pctrl, st.pctrl.data(), h->ndom * sizeof(PicardCtrl), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(P.diag, st.diag.data(), h->ndom * sizeof(DevDiag), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return DHARA_OK;
+}
+
+void fill_config(const dhara_handle *h, dhara_launch_config *out) {
+    std::memset(out, 0, sizeof(*out));
+    out->krylov_blocks_per_sm = h->L.krylov_per_sm;
+    out->overland_resident = h->L.olf_allow_resident;
+    out->overland_blocks_per_sm = h->L.olf_stream_per_sm;
+}
+
+}  // namespace
+
+int dhara_get_launch_config(dhara_handle *h, dhara_launch_config *out) {
+    if (!h || !out) return fail(DHARA_ERR_INVALID, "NULL argument");
+    fill_config(h, out);
+    return DHARA_OK;
+}
+
+int dhara_set_launch_config(dhara_handle *h, const dhara_launch_config *cfg) {
+    if (!h || !cfg) return fail(DHARA_ERR_INVALID, "NULL argument");
+    if (cfg->krylov_blocks_per_sm < 1 || cfg->krylov_blocks_per_sm > h->L.krylov_per_sm_max ||
+        cfg->overland_blocks_per_sm < 1 || cfg->overland_blocks_per_sm > h->L.olf_stream_per_sm_max)
+        return fail(DHARA_ERR_INVALID, "blocks per SM must be in [1, %d] (Krylov) and [1, %d] (overland)",
+                    h->L.krylov_per_sm_max, h->L.olf_stream_per_sm_max);
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->stream));
+    h->L.krylov_per_sm = cfg->krylov_blocks_per_sm;
+    h->L.olf_allow_resident = cfg->overland_resident ? 1 : 0;
+    h->L.olf_stream_per_sm = cfg->overland_blocks_per_sm;
+    if (h->graph_exec) {  // launch dimensions are baked into the graph
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    return DHARA_OK;
+}
+
+int dhara_autotune(dhara_handle *h, int trial_steps, dhara_launch_config *chosen) {
+    if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
+    if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
+    if (trial_steps < 1) trial_steps = 1;
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->stream));
+    SavedState st;
+    int rc = save_state(h, st);
+    if (rc) return rc;
+    const bool timing_was = h->timing;
+    double saved_ms[KT_N];
+    long long saved_n[KT_N];
+    collect_timing(h);
+    std::memcpy(saved_ms, h->total_ms, sizeof(saved_ms));
+    std::memcpy(saved_n, h->launches, sizeof(saved_n));
+    const long long saved_count = h->launch_count;
+    h->timing = true;
+    auto trial = [&](int kind, double *ms) -> int {
+        int r = restore_state(h, st);
+        if (r) return r;
+        collect_timing(h);
+        const double before = h->total_ms[kind];
+        for (int t = 0; t < trial_steps && !r; ++t) {
+            r = enqueue_subsurface(h);
+            if (!r) r = enqueue_overland(h);
+        }
+        if (r) return r;
+        CK(cudaStreamSynchronize(h->stream));
+        r = check_device_error(h);
+        if (r) return r;
+        collect_timing(h);
+        *ms = (h->total_ms[kind] - before) / trial_steps;
+        return DHARA_OK;
+    };
+    LaunchCfg &L = h->L;
+    // 3D Krylov: blocks per SM
+    int best_k = L.krylov_per_sm;
+    double best_kms = 1e300;
+    for (int b = 1; b <= L.krylov_per_sm_max && !rc; ++b) {
+        L.krylov_per_sm = b;
+        double ms = 0;
+        rc = trial(KT_KRYLOV, &ms);
+        if (!rc && ms < best_kms) { best_kms = ms; best_k = b; }
+    }
+    L.krylov_per_sm = best_k;
+    // overland: resident (when the segments fit) or streaming with b blocks per SM
+    int best_res = L.olf_allow_resident, best_ob = L.olf_stream_per_sm;
+    double best_oms = 1e300;
+    if (!rc && h->P.nseg <= L.olf_res_blocks) {
+        L.olf_allow_resident = 1;
+        double ms = 0;
+        rc = trial(KT_OLF_SOLVE, &ms);
+        if (!rc && ms < best_oms) { best_oms = ms; best_res = 1; }
+    }
+    for (int b = 1; b <= L.olf_stream_per_sm_max && !rc; ++b) {
+        L.olf_allow_resident = 0;
+        L.olf_stream_per_sm = b;
+        double ms = 0;
+        rc = trial(KT_OLF_SOLVE, &ms);
+        if (!rc && ms < best_oms) { best_oms = ms; best_res = 0; best_ob = b; }
+    }
+    L.olf_allow_resident = best_res;
+    L.olf_stream_per_sm = best_ob;
+    h->timing = timing_was;
+    const int rr = restore_state(h, st);
+    std::memcpy(h->total_ms, saved_ms, sizeof(saved_ms));
+    std::memcpy(h->launches, saved_n, sizeof(saved_n));
+    h->launch_count = saved_count;
+    if (h->graph_exec) {
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    if (rc) return rc;
+    if (rr) return rr;
+    if (chosen) {
+        fill_config(h, chosen);
+        chosen->krylov_ms = best_kms;
+        chosen->overland_ms = best_oms;
+    }
+    return DHARA_OK;
+}

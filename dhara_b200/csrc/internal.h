@@ -196,6 +196,11 @@ struct LaunchCfg {
     int coop_blocks_2d;
     int olf_res_blocks;    // co-resident blocks of the shared-memory-resident overland solve
     int olf_stream_blocks; // co-resident blocks of the streaming overland solve
+    // block schedule (dhara_autotune): blocks per SM actually launched
+    int sms;
+    int krylov_per_sm_max, krylov_per_sm;
+    int olf_stream_per_sm_max, olf_stream_per_sm;
+    int olf_allow_resident;
     int smem_3d;          // dynamic shared memory bytes of the 3D solve
     int nz_max;
     int mixed;

@@ -477,10 +477,11 @@ cudaError_t launch_overland_solve(const DevPtrs &P, const LaunchCfg &L, long lon
     DevPtrs args = P;
     long long c = ctot;
     void *kargs[] = {&args, &c};
-    if (P.nseg <= L.olf_res_blocks)
+    if (L.olf_allow_resident && P.nseg <= L.olf_res_blocks)
         return cudaLaunchCooperativeKernel((const void *)k_olf_pcg<true>, dim3(P.nseg), dim3(OLF_THREADS), kargs,
                                            OLF_RES_SMEM, s);
-    const int grid = L.olf_stream_blocks < P.nseg ? L.olf_stream_blocks : P.nseg;
+    const int blocks = L.olf_stream_per_sm * L.sms;
+    const int grid = blocks < P.nseg ? blocks : P.nseg;
     return cudaLaunchCooperativeKernel((const void *)k_olf_pcg<false>, dim3(grid), dim3(OLF_THREADS), kargs, 0, s);
 }
 
@@ -506,5 +507,8 @@ cudaError_t configure_2d(LaunchCfg &L, int device) {
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     L.olf_stream_blocks = per_sm * prop.multiProcessorCount;
     L.coop_blocks_2d = L.olf_stream_blocks;
+    L.olf_stream_per_sm_max = per_sm;
+    L.olf_stream_per_sm = per_sm;
+    L.olf_allow_resident = 1;
     return cudaSuccess;
 }

@@ -1140,7 +1140,8 @@ cudaError_t launch_dirichlet(const DevPtrs &P, const LaunchCfg &L, cudaStream_t 
 cudaError_t launch_krylov(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s) {
     DevPtrs args = P;
     void *kargs[] = {&args};
-    const int grid = L.coop_blocks_3d < P.ntiles ? L.coop_blocks_3d : P.ntiles;
+    const int blocks = L.krylov_per_sm * L.sms;
+    const int grid = blocks < P.ntiles ? blocks : P.ntiles;
     if (L.mixed)
         return cudaLaunchCooperativeKernel((const void *)k_krylov<float>, dim3(grid), dim3(TILE_THREADS),
                                            kargs, (size_t)L.smem_3d, s);
@@ -1164,6 +1165,9 @@ cudaError_t configure_3d(LaunchCfg &L, int device, int ntiles) {
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     L.coop_blocks_3d = per_sm * prop.multiProcessorCount;
+    L.sms = prop.multiProcessorCount;
+    L.krylov_per_sm_max = per_sm;
+    L.krylov_per_sm = per_sm;
     (void)ntiles;
     return cudaSuccess;
 }

@@ -246,6 +246,29 @@ int dhara_get_launch_count(dhara_handle *h, int64_t *count);
  * roofline figure divides by time), and the inner iterations they cover. */
 int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations);
 
+/* ---- block schedules ---------------------------------------------------------
+ * The persistent solvers' block schedules: how many co-resident blocks per SM
+ * the 3D Krylov solve launches (its tiles are strided over them), and whether
+ * the overland solve keeps each segment's vectors in shared memory (one block
+ * per segment, when they fit) or streams them with a given number of blocks
+ * per SM.  dhara_autotune times the candidates on this handle's own data --
+ * trial_steps steps per candidate from the current state, which it restores
+ * afterwards -- and keeps the fastest; *chosen (may be NULL) receives the
+ * result.  Defaults: the most blocks per SM that fit, overland resident when
+ * possible. */
+typedef struct {
+    int32_t krylov_blocks_per_sm;
+    int32_t overland_resident;
+    int32_t overland_blocks_per_sm;
+    int32_t pad;
+    double krylov_ms;     /* per trial step of the chosen schedule (autotune only) */
+    double overland_ms;
+} dhara_launch_config;
+
+int dhara_autotune(dhara_handle *h, int trial_steps, dhara_launch_config *chosen);
+int dhara_get_launch_config(dhara_handle *h, dhara_launch_config *out);
+int dhara_set_launch_config(dhara_handle *h, const dhara_launch_config *cfg);
+
 /* ---- output ----------------------------------------------------------------
  * The reference's outputs (SaveModelResults, src/io.cc:854-915, and
  * SaveResultEntirePeriod, src/io.cc:962-996) without its blocking per-step
