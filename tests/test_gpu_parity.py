@@ -217,8 +217,10 @@ def test_error_paths(gpu):
     with pytest.raises(db.DharaError) as e:
         s.upload("psi", np.zeros(3))
     assert e.value.code == 1
+    # Dirichlet faces are accepted, but the adjoint does not cover them
+    s.upload("bcw", np.zeros(d.params.nz * d.params.ny, np.int32))
     with pytest.raises(db.DharaError) as e:
-        s.upload("bcw", np.zeros(d.params.nz * d.params.ny, np.int32))
+        s.adjoint(np.zeros((1, 3, d.params.nx * d.params.ny)), np.zeros(1), 1)
     assert e.value.code == 4
     with pytest.raises(db.DharaError) as e:
         s.upload("ksat", np.full(d.ncells, np.nan))
