@@ -22,6 +22,8 @@
 #define CHUNK_F32 4
 #define CHUNK_F64 2
 #define CH_R 2
+// TMA staging buffers per block (chunks in flight ahead of the one being computed: STAGES - 1)
+#define STAGES 2
 
 // Tensor maps of one domain (index = dom * NMAP + id): halo boxes
 // (TILE_X + 32 bytes) x (TILE_Y + 2) x chunk, own boxes TILE_X x TILE_Y x chunk.

@@ -106,6 +106,13 @@ template <typename V, int CHN>
 constexpr unsigned own_bytes() {
     return (unsigned)(CHN * OWN_PLANE * sizeof(V));
 }
+// Stride of a halo box's slot in a staging buffer: the TMA writes shared
+// memory at 128-byte aligned addresses, so each slot is the box's bytes
+// rounded up to 128 (the transaction count stays halo_bytes).
+template <typename V, int CHN>
+constexpr unsigned halo_slot() {
+    return (halo_bytes<V, CHN>() + 127u) & ~127u;
+}
 
 // Block-uniform state of the two staging buffers: mbarriers and the parity
 // each buffer's next completion will have.

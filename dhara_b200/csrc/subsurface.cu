@@ -396,52 +396,51 @@ struct Chunk {
     static constexpr int inner = sizeof(T) == 4 ? CHUNK_F32 : CHUNK_F64;
 };
 
-// Bytes of one staging buffer of each phase (the kernel reserves two buffers
+// Bytes of one staging buffer of each phase (the kernel reserves STAGES buffers
 // of the largest).
 template <typename T>
 struct StageSize {
     static constexpr int C = Chunk<T>::inner;
     // phase A: z, p_old, K (halo); D (own)
-    static constexpr size_t A = 3 * (size_t)halo_bytes<T, C>() + own_bytes<T, C>();
+    static constexpr size_t A = 3 * (size_t)halo_slot<T, C>() + own_bytes<T, C>();
     // phase B: p, q, d, r, 1/den, a/den (own)
     static constexpr size_t B = 6 * (size_t)own_bytes<T, C>();
     // phase R: x, K64 (halo); D64, b (own), all FP64
-    static constexpr size_t R = 2 * (size_t)halo_bytes<double, CH_R>() + 2 * (size_t)own_bytes<double, CH_R>();
+    static constexpr size_t R = 2 * (size_t)halo_slot<double, CH_R>() + 2 * (size_t)own_bytes<double, CH_R>();
     static constexpr size_t buffer() { return A > B ? (A > R ? A : R) : (B > R ? B : R); }
-    static constexpr size_t bytes() { return 2 * buffer(); }
+    static constexpr size_t bytes() { return STAGES * buffer(); }
 };
 
 // Chunked march over a tile's planes: thread 0 arms and issues chunk st into
-// buffer st & 1 (issue(st, b)); every thread waits for the chunk and computes
-// its planes (plane(b, pl, k)).  With NEXT, the last plane of a chunk also reads
-// the first plane of the next chunk (the z-neighbour of a stencil), which is
-// awaited first.  A buffer is refilled with chunk st + 2 once all threads are
-// done with it; when the tile is done, issue_next() starts the block's next
-// tile so its first chunks stream in during this tile's epilogue.
+// buffer st % STAGES (issue(st, b)), so STAGES - 1 chunks are in flight while
+// one is computed; every thread waits for the chunk and computes its planes
+// (plane(b, pl, k)).  With NEXT, the last plane of a chunk also reads the first
+// plane of the next chunk (the z-neighbour of a stencil), which is awaited
+// first.  A buffer is refilled with chunk st + STAGES once all threads are done
+// with it; when the tile is done, issue_next() starts the block's next tile so
+// its first chunks stream in during this tile's epilogue.
 template <int CHN, bool NEXT, typename Issue, typename PlaneFn, typename NextFn>
 __device__ __forceinline__ void march(int nz, StageBars &sb, bool prefetched, Issue issue, PlaneFn plane,
                                       NextFn issue_next) {
     const int nst = (nz + CHN - 1) / CHN;
-    if (threadIdx.x == 0 && !prefetched) {
-        issue(0, 0);
-        if (nst > 1) issue(1, 1);
-    }
+    if (threadIdx.x == 0 && !prefetched)
+        for (int q = 0; q < STAGES && q < nst; ++q) issue(q, q);
     bool next_ready = false;
     for (int st = 0; st < nst; ++st) {
-        const int b = st & 1;
+        const int b = st % STAGES;
         if (!next_ready) sb.wait(b);
         next_ready = false;
         for (int pl = 0; pl < CHN; ++pl) {
             const int k = st * CHN + pl;
             if (k >= nz) break;
             if (NEXT && pl == CHN - 1 && k + 1 < nz) {
-                sb.wait(b ^ 1);
+                sb.wait((b + 1) % STAGES);
                 next_ready = true;
             }
             plane(b, pl, k);
         }
         __syncthreads();
-        if (threadIdx.x == 0 && st + 2 < nst) issue(st + 2, b);
+        if (threadIdx.x == 0 && st + STAGES < nst) issue(st + STAGES, b);
     }
     if (threadIdx.x == 0) issue_next();
 }
@@ -515,23 +514,26 @@ template <typename T>
 __device__ __forceinline__ void issue_R(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
                                         StageBars &sb) {
     constexpr int CHN = CH_R;
-    constexpr unsigned HB = halo_bytes<double, CHN>(), OB = own_bytes<double, CHN>();
+    constexpr unsigned HB = halo_bytes<double, CHN>(), HS = halo_slot<double, CHN>();
+    constexpr unsigned OB = own_bytes<double, CHN>();
+    static_assert(HS % 128 == 0 && OB % 128 == 0, "TMA destinations must be 128-byte aligned");
     const TileDesc td = P.tiles[tile];
     const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
     unsigned char *B = stage + b * StageSize<T>::buffer();
     const int k0 = st * CHN;
     mbar_expect_tx(sb.bar + b, 2 * HB + 2 * OB);
     tma_halo<double, CHN>((double *)B, maps + MAP_X64_H, td.x0, td.y0, k0, sb.bar + b);
-    tma_halo<double, CHN>((double *)(B + HB), maps + MAP_K64_H, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<double, CHN>((double *)(B + 2 * HB), maps + MAP_D64_O, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<double, CHN>((double *)(B + 2 * HB + OB), maps + MAP_B_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_halo<double, CHN>((double *)(B + HS), maps + MAP_K64_H, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<double, CHN>((double *)(B + 2 * HS), maps + MAP_D64_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<double, CHN>((double *)(B + 2 * HS + OB), maps + MAP_B_O, td.x0, td.y0, k0, sb.bar + b);
 }
 
 template <typename T>
 __device__ __forceinline__ void issue_A(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
                                         StageBars &sb, bool first, int parity_old) {
     constexpr int CHN = Chunk<T>::inner;
-    constexpr unsigned HB = halo_bytes<T, CHN>(), OB = own_bytes<T, CHN>();
+    constexpr unsigned HB = halo_bytes<T, CHN>(), HS = halo_slot<T, CHN>(), OB = own_bytes<T, CHN>();
+    static_assert(HS % 128 == 0 && OB % 128 == 0, "TMA destinations must be 128-byte aligned");
     const TileDesc td = P.tiles[tile];
     const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
     unsigned char *B = stage + b * StageSize<T>::buffer();
@@ -539,9 +541,9 @@ __device__ __forceinline__ void issue_A(const DevPtrs &P, int tile, int st, int 
     mbar_expect_tx(sb.bar + b, (first ? 2 : 3) * HB + OB);
     tma_halo<T, CHN>((T *)B, maps + MAP_Z_H, td.x0, td.y0, k0, sb.bar + b);
     if (!first)
-        tma_halo<T, CHN>((T *)(B + HB), maps + (parity_old ? MAP_P1_H : MAP_P0_H), td.x0, td.y0, k0, sb.bar + b);
-    tma_halo<T, CHN>((T *)(B + 2 * HB), maps + MAP_K_H, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<T, CHN>((T *)(B + 3 * HB), maps + MAP_D_O, td.x0, td.y0, k0, sb.bar + b);
+        tma_halo<T, CHN>((T *)(B + HS), maps + (parity_old ? MAP_P1_H : MAP_P0_H), td.x0, td.y0, k0, sb.bar + b);
+    tma_halo<T, CHN>((T *)(B + 2 * HS), maps + MAP_K_H, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + 3 * HS), maps + MAP_D_O, td.x0, td.y0, k0, sb.bar + b);
 }
 
 template <typename T>
@@ -565,8 +567,7 @@ __device__ __forceinline__ void issue_B(const DevPtrs &P, int tile, int st, int 
 // Issues chunks 0 and 1 of a tile (the prefetch of the block's next tile).
 template <int CHN, typename Issue>
 __device__ __forceinline__ void issue_head(int nz, Issue issue) {
-    issue(0, 0);
-    if (nz > CHN) issue(1, 1);
+    for (int q = 0; q < STAGES && q * CHN < nz; ++q) issue(q, q);
 }
 
 // ---- phase R: outer FP64 residual and the preconditioner factors -------------
@@ -579,7 +580,7 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
                         const StencilW<T> &w, T *s_d, unsigned char *stage, StageBars &sb, double (&v)[3]) {
     constexpr int CHN = CH_R;
     typedef Halo<double> H;
-    constexpr unsigned HB = halo_bytes<double, CHN>(), OB = own_bytes<double, CHN>();
+    constexpr unsigned HB = halo_slot<double, CHN>(), OB = own_bytes<double, CHN>();
     T *__restrict__ r = (T *)P.r;
     T *__restrict__ z = (T *)P.z;
     T *__restrict__ finv = (T *)P.finv;
@@ -608,7 +609,7 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
         double x_dn = 0.0, K_dn = 0.0;
         if (k + 1 < nz) {
             if (pl + 1 < CHN) { x_dn = sx[H::PLANE + hc]; K_dn = sK[H::PLANE + hc]; }
-            else { x_dn = ((const double *)buf(b ^ 1))[hc]; K_dn = ((const double *)(buf(b ^ 1) + HB))[hc]; }
+            else { x_dn = ((const double *)buf((b + 1) % STAGES))[hc]; K_dn = ((const double *)(buf((b + 1) % STAGES) + HB))[hc]; }
         }
         const double mu = k > 0 ? 1.0 : 0.0, md = k < nz - 1 ? 1.0 : 0.0;
         const double Kw = sK[hc - 1], Ke = sK[hc + 1], Ks = sK[hc - H::BW], Kn = sK[hc + H::BW];
@@ -663,7 +664,7 @@ __device__ void phase_A(const DevPtrs &P, int tile, int tile_next, bool prefetch
                         double (&v)[1]) {
     constexpr int CHN = Chunk<T>::inner;
     typedef Halo<T> H;
-    constexpr unsigned HB = halo_bytes<T, CHN>();
+    constexpr unsigned HB = halo_slot<T, CHN>();
     T *__restrict__ q = (T *)P.q;
     const size_t BUF = StageSize<T>::buffer();
     auto buf = [&](int b) { return stage + b * BUF; };
@@ -691,9 +692,9 @@ __device__ void phase_A(const DevPtrs &P, int tile, int tile_next, bool prefetch
         if (k + 1 < nz) {
             if (pl + 1 < CHN) { p_dn = pv(sz + H::PLANE, sq + H::PLANE, hc); K_dn = sK[H::PLANE + hc]; }
             else {
-                const T *nz_ = (const T *)buf(b ^ 1), *nq = (const T *)(buf(b ^ 1) + HB);
+                const T *nz_ = (const T *)buf((b + 1) % STAGES), *nq = (const T *)(buf((b + 1) % STAGES) + HB);
                 p_dn = pv(nz_, nq, hc);
-                K_dn = ((const T *)(buf(b ^ 1) + 2 * HB))[hc];
+                K_dn = ((const T *)(buf((b + 1) % STAGES) + 2 * HB))[hc];
             }
         }
         const T Kc = sK[hc];
@@ -797,17 +798,16 @@ __device__ __forceinline__ void stop_inner(const DevPtrs &P, KrylovCtrl &c) {
 template <typename T>
 __global__ void __launch_bounds__(TILE_THREADS) k_krylov(DevPtrs P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ __align__(8) uint64_t s_bar[STAGES];
     constexpr bool DSMEM = sizeof(T) == 4;
-    // dynamic shared memory: [d' of the column solves (float only)][two staging
-    // buffers], the staging buffers 128-byte aligned for the TMA
+    // dynamic shared memory: [d' of the column solves (float only)][STAGES
+    // staging buffers], the staging buffers 128-byte aligned for the TMA
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
     T *s_d = reinterpret_cast<T *>(base);
     const size_t dprime_bytes = DSMEM ? (size_t)P.smem_nz * TILE_THREADS * sizeof(T) : 0;
     unsigned char *stage_raw = base + ((dprime_bytes + 127) & ~(size_t)127);
     if (threadIdx.x == 0) {
-        mbar_init(&s_bar[0], 1);
-        mbar_init(&s_bar[1], 1);
+        for (int q = 0; q < STAGES; ++q) mbar_init(&s_bar[q], 1);
         mbar_fence_init();
     }
     __syncthreads();
