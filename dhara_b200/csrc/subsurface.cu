@@ -145,8 +145,10 @@ __global__ void k_prologue(DevPtrs P) {
 // terms of SetUpBoundaryConditionsSubsurface (126-353) in the reference's
 // order top, bottom, south, north, west, east; the bottom is free drainage
 // (q_b = K of the bottom cell, written to bcqb as the reference does).
+// Eight blocks per SM (64 registers): the FP64 closure's latency chains need the
+// warps more than the registers (measured 18 % faster than the uncapped 96).
 template <typename T>
-__global__ void __launch_bounds__(TILE_THREADS) k_assemble(DevPtrs P) {
+__global__ void __launch_bounds__(TILE_THREADS, 8) k_assemble(DevPtrs P) {
     const int tile = blockIdx.x;
     const TileDesc td = P.tiles[tile];
     const DomainDesc &D = P.dom[td.dom];
