@@ -304,6 +304,9 @@ def run_ours(args, world, rank, local):
                 "algorithmic_bytes_per_launch": kbytes / kn if kn else None,
                 "avg_launch_ms": kms / kn if kn else None,
                 "launches": kn, "share_of_step": kms / ms if ms else None}
+    # the storm's Krylov work depends on the chaotic Picard trajectory, so the
+    # kernel's speed is also given per inner (FP32 CG) iteration
+    krylov_ms_per_inner = kms / kiters if kiters else None
 
     adjoint = run_adjoint(args, local) if args.adjoint_steps > 0 else None
     ensemble = run_ensemble(args, local) if args.ensemble_steps > 0 else None
@@ -325,6 +328,7 @@ def run_ours(args, world, rank, local):
         "mass_error_over_inflow": mass_err / inflow if inflow else None,
         "picard_iters": dg["picard_iters_total"], "krylov_inner_iters": dg["krylov_iters_total"],
         "refine_cycles": dg["refine_iters_total"], "overland_iters": dg["overland_iters_total"],
+        "krylov_ms_per_inner_iter": krylov_ms_per_inner,
         "adjoint_over_forward": adjoint["adjoint_over_forward"] if adjoint else None,
         "adjoint": adjoint,
         "ensemble": ensemble,

@@ -373,7 +373,7 @@ int build_tensor_maps(dhara_handle *h) {
         rc |= encode_map(m + MAP_P1_O, P.p1, sT, D, false, chi);
         rc |= encode_map(m + MAP_Q_O, P.q, sT, D, false, chi);
         rc |= encode_map(m + MAP_INV_O, P.finv, sT, D, false, chi);
-        rc |= encode_map(m + MAP_E_O, P.fe, sT, D, false, chi);
+        rc |= encode_map(m + MAP_C_O, P.fc, sT, D, false, chi);
         rc |= encode_map(m + MAP_X64_H, P.x, 8, D, true, CH_R);
         rc |= encode_map(m + MAP_K64_H, P.K64, 8, D, true, CH_R);
         rc |= encode_map(m + MAP_D64_O, P.D64, 8, D, false, CH_R);
@@ -623,7 +623,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     TileDesc *d_tiles = nullptr;
     rc |= dalloc(h, &d_tiles, h->htiles.size());
     for (double **q : {&P.psin, &P.thetan, &P.psim, &P.x, &P.b, &P.ksat}) rc |= dalloc(h, q, N);
-    for (void **q : {&P.K, &P.D, &P.r, &P.p0, &P.p1, &P.z, &P.d, &P.q, &P.finv, &P.fe, &P.fc})
+    for (void **q : {&P.K, &P.D, &P.r, &P.p0, &P.p1, &P.z, &P.d, &P.q, &P.finv, &P.fc})
         rc |= dalloc_void(h, q, N * sT);
     if (h->mixed) {
         rc |= dalloc(h, &P.K64, N);
@@ -686,7 +686,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     auto zero = [&](void *p, size_t bytes) { return cudaMemsetAsync(p, 0, bytes, h->stream); };
     cudaError_t e = cudaSuccess;
     for (double *q : {P.psin, P.thetan, P.psim, P.x, P.b, P.ksat}) e = e ? e : zero(q, N * 8);
-    for (void *q : {P.K, P.D, P.r, P.p0, P.p1, P.z, P.d, P.q, P.finv, P.fe, P.fc}) e = e ? e : zero(q, N * sT);
+    for (void *q : {P.K, P.D, P.r, P.p0, P.p1, P.z, P.d, P.q, P.finv, P.fc}) e = e ? e : zero(q, N * sT);
     for (double *q : {P.K64, P.D64}) e = e ? e : zero(q, N * 8);
     for (double *q : {P.ztopo, P.mann, P.h, P.H, P.ph, P.ppt, P.esoil, P.tr, P.hpoten, P.qtop, P.ktop, P.bcqb,
                       P.olf_b, P.olf_r, P.olf_p0, P.olf_p1, P.olf_z, P.olf_w, P.olf_s, P.olf_p})
@@ -1163,10 +1163,11 @@ int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations
         const double cycles = (double)dg.refine_iters_total;
         const double upd = cycles > solves ? cycles - solves : 0.0;
         // inner iteration: phase A reads z, p_old, K, D and writes p, q (6 T-words);
-        // phase B reads p, q, d, r, 1/den, a/den, c/den and writes d, r, z (10);
-        // outer residual R: x, b, K64, D64 (f64) + writes r, z and the three
-        // factors (5 T) + c/den read back (1 T); update U: x read+write (f64) + d (T).
-        total += N * (16.0 * sT * (double)dg.krylov_iters_total + (32.0 + 6.0 * sT) * cycles +
+        // phase B reads p, q, d, r, 1/den, c' and writes d, r, z (9; the back
+        // sweep's second read of c' follows the staged read and is not counted);
+        // outer residual R: x, b, K64, D64 (f64) + writes r, z and the two
+        // factors (4 T) + c' read back (1 T); update U: x read+write (f64) + d (T).
+        total += N * (15.0 * sT * (double)dg.krylov_iters_total + (32.0 + 5.0 * sT) * cycles +
                       (16.0 + sT) * upd);
         iters += dg.krylov_iters_total;
     }

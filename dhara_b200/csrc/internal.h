@@ -19,7 +19,7 @@
 #define TILE_THREADS (TILE_X * TILE_Y)
 #define NZ_MAX 64
 // planes per TMA-staged chunk: inner phases (by inner precision) and the FP64 residual
-#define CHUNK_F32 4
+#define CHUNK_F32 3
 #define CHUNK_F64 2
 #define CH_R 2
 // TMA staging buffers per block (chunks in flight ahead of the one being computed: STAGES - 1)
@@ -30,7 +30,7 @@
 enum {
     MAP_P0_H = 0, MAP_P1_H, MAP_Z_H, MAP_K_H,      // inner precision, halo boxes
     MAP_D_O, MAP_DD_O, MAP_R_O,                    // inner precision, own boxes (D, d, r)
-    MAP_P0_O, MAP_P1_O, MAP_Q_O, MAP_INV_O, MAP_E_O,  // inner precision, own boxes
+    MAP_P0_O, MAP_P1_O, MAP_Q_O, MAP_INV_O, MAP_C_O,  // inner precision, own boxes
     MAP_X64_H, MAP_K64_H, MAP_D64_O, MAP_B_O,      // FP64 outer residual
     NMAP
 };
@@ -159,8 +159,8 @@ struct DevPtrs {
     // 3D inner-precision buffers
     void *K, *D, *r, *p0, *p1, *z, *d;
     // A p of the current direction, and the column preconditioner's stored
-    // Thomas factors (1/den, a/den, c/den), computed once per outer cycle
-    void *q, *finv, *fe, *fc;
+    // L D L^T factors (1/den, c' = c/den), computed once per outer cycle
+    void *q, *finv, *fc;
     // 2D double
     double *ztopo, *mann, *h, *H, *ph, *ppt, *esoil, *tr, *hpoten, *qtop, *ktop, *bcqb;
     double *olf_k;       // 4*C: kw, ke, ks, kn per column (row-based)

@@ -405,7 +405,7 @@ struct StageSize {
     static constexpr int C = Chunk<T>::inner;
     // phase A: z, p_old, K (halo); D (own)
     static constexpr size_t A = 3 * (size_t)halo_slot<T, C>() + own_bytes<T, C>();
-    // phase B: p, q, d, r, 1/den, a/den (own)
+    // phase B: p, q, d, r, 1/den, c' (own)
     static constexpr size_t B = 6 * (size_t)own_bytes<T, C>();
     // phase R: x, K64 (halo); D64, b (own), all FP64
     static constexpr size_t R = 2 * (size_t)halo_slot<double, CH_R>() + 2 * (size_t)own_bytes<double, CH_R>();
@@ -448,15 +448,20 @@ __device__ __forceinline__ void march(int nz, StageBars &sb, bool prefetched, Is
 }
 
 // The column preconditioner M is the z-coupled (tridiagonal) part of A:
-// b_k = D_k + sum_f w_f k_f, a_k = -w_z kd_k, c_k = -w_z ku_k.  It is factored
-// once per outer cycle (phase R) by the Thomas algorithm,
+// b_k = D_k + sum_f w_f k_f, a_k = -w_z kd_k, c_k = -w_z ku_k.  The column is
+// symmetric (a_{k+1} = c_k: both are -w_z (K_k + K_{k+1}) / 2 from the same
+// rounded operands), so M = L D L^T with D = diag(den) and the unit lower
+// bidiagonal L of l_{k+1} = c_k / den_k = c'_k.  It is factored once per outer
+// cycle (phase R),
 //   den_k = b_k - a_k c'_{k-1},  c'_k = c_k / den_k,
-// and the factors 1/den, e = a/den and c' are stored per cell, so applying M^-1
-// in the inner iterations is two FMA recurrences:
-//   forward  d'_k = r_k / den_k - e_k d'_{k-1},  backward z_k = d'_k - c'_k z_{k+1}.
-// With M = L D L^T (D = den), r^T M^-1 r = sum_k den_k d'_k^2 is accumulated in
-// the forward sweep.  d' lives in shared memory when T is float (DSMEM), else
-// in the z array itself.
+// and only 1/den and c' are stored per cell.  Applying M^-1 in the inner
+// iterations is three short recurrences:
+//   forward  y_k = r_k - c'_{k-1} y_{k-1},  d'_k = y_k / den_k,
+//   backward z_k = d'_k - c'_k z_{k+1},
+// and r^T M^-1 r = sum_k y_k d'_k is accumulated in the forward sweep.  Any
+// rounding of the stored factors still gives a symmetric M (the same c' feeds
+// both sweeps), so the inner CG sees a fixed SPD preconditioner.  d' lives in
+// shared memory when T is float (DSMEM), else in the z array itself.
 template <typename T, bool DSMEM>
 __device__ __forceinline__ void put_dprime(T dp, T *s_d, int k, T *__restrict__ zg) {
     if (DSMEM) s_d[k * TILE_THREADS + threadIdx.x] = dp;
@@ -563,7 +568,7 @@ __device__ __forceinline__ void issue_B(const DevPtrs &P, int tile, int st, int 
     if (!first) tma_own<T, CHN>((T *)(B + 2 * OB), maps + MAP_DD_O, td.x0, td.y0, k0, sb.bar + b);
     tma_own<T, CHN>((T *)(B + 3 * OB), maps + MAP_R_O, td.x0, td.y0, k0, sb.bar + b);
     tma_own<T, CHN>((T *)(B + 4 * OB), maps + MAP_INV_O, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<T, CHN>((T *)(B + 5 * OB), maps + MAP_E_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + 5 * OB), maps + MAP_C_O, td.x0, td.y0, k0, sb.bar + b);
 }
 
 // Issues chunks 0 and 1 of a tile (the prefetch of the block's next tile).
@@ -574,8 +579,8 @@ __device__ __forceinline__ void issue_head(int nz, Issue issue) {
 
 // ---- phase R: outer FP64 residual and the preconditioner factors -------------
 // r = b - A x with the FP64 coefficients, r_T = (T) r; the column factors of M
-// from the inner operator's T coefficients (the same rounding as the stored
-// K, D) are stored; z = M^-1 r_T; v = {||r||^2, ||b||^2, r.z}.
+// (1/den and c') from the inner operator's T coefficients (the same rounding as
+// the stored K, D) are stored; z = M^-1 r_T; v = {||r||^2, ||b||^2, r.z}.
 // Staged: x, K64 (halo), D64, b (own).
 template <typename T, bool DSMEM>
 __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetched, const ColumnRef &cr,
@@ -586,7 +591,6 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
     T *__restrict__ r = (T *)P.r;
     T *__restrict__ z = (T *)P.z;
     T *__restrict__ finv = (T *)P.finv;
-    T *__restrict__ fe = (T *)P.fe;
     T *__restrict__ fc = (T *)P.fc;
     const size_t BUF = StageSize<T>::buffer();
     auto buf = [&](int b) { return stage + b * BUF; };
@@ -600,7 +604,7 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
     const Masks M = masks_of(cr);
     const double cx = (double)w.cx, cy = (double)w.cy, cz = (double)w.cz;
     double x_up = 0.0, K_up = 0.0;
-    T cprev = T(0), dprev = T(0);
+    T cprev = T(0), yprev = T(0);
     auto plane = [&](int b, int pl, int k) {
         if (!cr.valid) return;
         const double *sx = (const double *)buf(b) + pl * H::PLANE;
@@ -639,15 +643,15 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
         const T a = -w.cz * kdT, c = -w.cz * kuT;
         const T den = bd - a * cprev;
         const T inv = fixed ? T(0) : recip(den);
-        const T cp = c * inv, e = a * inv;
-        const T dp = rT * inv - e * dprev;
+        const T cp = c * inv;
+        const T y = rT - cprev * yprev;
+        const T dp = y * inv;
         finv[g] = inv;
-        fe[g] = e;
         fc[g] = cp;
         put_dprime<T, DSMEM>(dp, s_d, k, z + g);
-        if (!fixed) v[2] += (double)den * (double)dp * (double)dp;
+        v[2] += (double)y * (double)dp;
         cprev = cp;
-        dprev = dp;
+        yprev = y;
         x_up = xc;
         K_up = Kc;
     };
@@ -742,22 +746,24 @@ __device__ void phase_B(const DevPtrs &P, int tile, int tile_next, bool prefetch
             });
     };
     const int nz = cr.nz, oc = threadIdx.x;
-    T dprev = T(0);
+    T cprev = T(0), yprev = T(0);
     auto plane = [&](int b, int pl, int k) {
         if (!cr.valid) return;
         const T *B = (const T *)buf(b) + pl * OWN_PLANE + oc;
         constexpr int S = CHN * OWN_PLANE;
         const T pc = B[0], qc = B[S], dold = first ? T(0) : B[2 * S], rold = B[3 * S];
-        const T inv = B[4 * S], e = B[5 * S];
+        const T inv = B[4 * S], cp = B[5 * S];
         const long long g = cr.g0 + (long long)k * cr.sxy;
         d[g] = dold + alpha * pc;
         const T rk = rold - alpha * qc;
         r[g] = rk;
         v[0] += (double)rk * (double)rk;
-        const T dp = rk * inv - e * dprev;
+        const T y = rk - cprev * yprev;
+        const T dp = y * inv;
         put_dprime<T, DSMEM>(dp, s_d, k, z + g);
-        if (inv != T(0)) v[1] += (double)dp * (double)dp / (double)inv;
-        dprev = dp;
+        v[1] += (double)y * (double)dp;
+        cprev = cp;
+        yprev = y;
     };
     march<CHN, false>(nz, sb, prefetched, issue, plane, issue_next);
     (void)OB;
@@ -798,7 +804,7 @@ __device__ __forceinline__ void stop_inner(const DevPtrs &P, KrylovCtrl &c) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(TILE_THREADS) k_krylov(DevPtrs P) {
+__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 1) k_krylov(DevPtrs P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar[STAGES];
     constexpr bool DSMEM = sizeof(T) == 4;
