@@ -5,7 +5,7 @@
 // SubsurfaceFlowModel then OverlandFlowModel, src/device.cu:450-458) is a
 // fixed launch sequence with no host synchronisation:
 //   k_prologue; [k_assemble, k_krylov (persistent), k_picard_check] x maxiter;
-//   k_epilogue; k_olf_setup, k_olf_pcg (persistent), k_olf_finish
+//   k_epilogue; k_olf_setup, k_olf_pcg_res or k_olf_pcg (persistent), k_olf_finish
 // Domains whose Picard loop has converged skip the remaining iterations on the
 // device, so the sequence can be captured once into a CUDA graph and replayed.
 #include "internal.h"

@@ -137,7 +137,7 @@ struct GlobalCtrl {
     int n_active;        // domains with an active outer solve
     int n_inner_active;  // domains with an active inner solve
     int n_olf_active;
-    int pad;
+    unsigned int olf_bar;  // arrivals at the resident overland solve's barrier
     int olf_live[4];     // domains still iterating, rotating over three phases
 };
 

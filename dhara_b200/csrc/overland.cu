@@ -3,7 +3,7 @@
 //
 //   WaterElevationOverland (33-45) + UpdateKOverland (193-368)
 //     + SetUpLinearSystemsOverland (65-189)                  -> k_olf_setup
-//   CUSP CG on the 5-diagonal matrix (410-411)               -> k_olf_pcg
+//   CUSP CG on the 5-diagonal matrix (410-411)               -> k_olf_pcg_res / k_olf_pcg
 //   WaterDepthOverland (371-383) + ph <- waterdepth (417)     -> k_olf_finish
 //
 // The boundary ring is a fixed-elevation (identity) row in the reference.  Its
@@ -42,6 +42,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_olf_setup(DevPtrs P, long long
         P.gctrl->olf_live[0] = 0;
         P.gctrl->olf_live[1] = 0;
         P.gctrl->olf_live[2] = 0;
+        P.gctrl->olf_bar = 0;
     }
     const ColumnRef cr = column_of(P, tile);
     if (!cr.valid) return;
@@ -119,11 +120,10 @@ __device__ __forceinline__ double olf_apply(const OlfRow &w, const ColumnRef &cr
 // barrier.  The fixed ring is eliminated (its values stay H_old).
 //
 // Vectors: x (= H), r, w = A u, z = A q, s = A p, p, with u = r/diag and
-// q = s/diag formed on the fly; m alternates between two buffers.  In the
-// resident variant (RES) each block owns one segment for the whole solve and
-// keeps x, r, w, z, s, p, m and the row coefficients in shared memory; only m
-// goes through global memory (for the neighbours) and x is written back when
-// the domain stops.
+// q = s/diag formed on the fly; m alternates between two buffers.  Two
+// variants: k_olf_pcg_res (one resident block per segment) and k_olf_pcg
+// (blocks loop over segments); both do the same arithmetic in the same order,
+// so their results agree bit for bit.
 
 template <int NV>
 __device__ __forceinline__ void olf_block_sum(double (&v)[NV]) {
@@ -198,18 +198,127 @@ __device__ __forceinline__ OlfCoef olf_coef(const DevPtrs &P, const DomainDesc &
     return k;
 }
 
+__device__ __forceinline__ double olf_av4(const OlfCoef &k, double vc, double vw, double ve, double vs, double vn) {
+    return k.dg * vc - ((k.ce * ve + k.cw * vw) + (k.cn * vn + k.cs * vs));
+}
+
 template <bool CG>
 __device__ __forceinline__ double olf_av(const OlfCoef &k, const double *v, long long c, int nx, double vc) {
     const double vw = CG ? __ldcg(v + c - 1) : v[c - 1];
     const double ve = CG ? __ldcg(v + c + 1) : v[c + 1];
     const double vs = CG ? __ldcg(v + c - nx) : v[c - nx];
     const double vn = CG ? __ldcg(v + c + nx) : v[c + nx];
-    return k.dg * vc - ((k.ce * ve + k.cw * vw) + (k.cn * vn + k.cs * vs));
+    return olf_av4(k, vc, vw, ve, vs, vn);
 }
 
-template <bool RES>
+// Vectors of one interior row carried by the pipelined recurrence.
+struct OlfVec {
+    double x, r, w, z, s, p;
+};
+
+// One iteration's vector updates at a row (Ghysels & Vanroose, Alg. 4): n is
+// (A m)_c, the previous z, s, p are in e unless first.  Adds this row's
+// gamma = r.u, delta = w.u and r.r terms to v and returns m = w/diag.
+__device__ __forceinline__ double olf_update(OlfVec &e, double dg, double n, double alpha, double beta,
+                                             bool first, double (&v)[3]) {
+    const double u = e.r / dg;
+    if (first) {
+        e.z = n;
+        e.s = e.w;
+        e.p = u;
+    } else {
+        e.z = n + beta * e.z;
+        e.s = e.w + beta * e.s;
+        e.p = u + beta * e.p;
+    }
+    e.x += alpha * e.p;
+    e.r -= alpha * e.s;
+    e.w -= alpha * e.z;
+    const double un = e.r / dg;
+    v[0] += e.r * un;
+    v[1] += e.w * un;
+    v[2] += e.r * e.r;
+    return e.w / dg;
+}
+
+// Stop test and step lengths of iteration it for segment s (one thread).
+// dsum = the domain's (gamma, delta, r.r).  Returns 1 to iterate, with alpha,
+// beta and the carried gamma_prev, alpha_prev updated, and counts the domain
+// as live for the next iteration; on a stop the domain's first segment
+// records the iteration count and residual.
+__device__ __forceinline__ int olf_decide(const DevPtrs &P, int s, const OlfSeg &sg, const DomainDesc &D, int it,
+                                          const double (&dsum)[3], double bb, double &gamma_prev,
+                                          double &alpha_prev, double &alpha, double &beta) {
+    const double gam = dsum[0], del = dsum[1], rr = dsum[2];
+    const double tol2 = D.overland_tol * D.overland_tol;
+    bool stop = rr <= tol2 * bb;
+    stop = stop || it >= D.overland_maxiter || !(rr == rr) || !(gam == gam);
+    alpha = 0.0;
+    beta = 0.0;
+    if (!stop) {
+        if (it == 0) {
+            alpha = gam / del;
+        } else {
+            beta = gam / gamma_prev;
+            alpha = gam / (del - beta * gam / alpha_prev);
+        }
+        if (!(alpha > 0.0) || !(alpha < 1e300)) stop = true;  // breakdown
+    }
+    if (stop) {
+        if (s == sg.first) {
+            OverlandCtrl &oc = P.octrl[sg.dom];
+            oc.iter = it;
+            oc.rr = rr;
+            oc.bb = bb;
+        }
+        return 0;
+    }
+    gamma_prev = gam;
+    alpha_prev = alpha;
+    if (s == sg.first) atomicAdd(&P.gctrl->olf_live[(it + 1) % 3], 1);
+    return 1;
+}
+
+// Grid barrier of the resident overland solve: a counter that every block
+// adds one to (a release reduction) and polls until it reaches target =
+// epoch x blocks (acquire loads), so no block has to reset anything between
+// barriers; k_olf_setup zeroes it before each solve.  Bounded like grid_sync:
+// a wait beyond BARRIER_TIMEOUT_NS, or an error raised by another block, sets
+// or reads GridBarrier::error and returns false in every thread.
+__device__ __forceinline__ bool olf_sync(unsigned int *count, unsigned int target, GridBarrier *gb) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
+        const unsigned long long t0 = global_ns();
+        unsigned int spins = 0;
+        for (;;) {
+            unsigned int v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+            if ((int)(v - target) >= 0) break;
+            if ((++spins & 63u) == 0) {
+                if (*(volatile int *)&gb->error) {
+                    ok = 0;
+                    break;
+                }
+                if (global_ns() - t0 > BARRIER_TIMEOUT_NS) {
+                    atomicExch(&gb->error, 1);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Streaming variant: blocks loop over segments (more segments than resident
+// blocks); the vectors live in global memory and the segment scalars in
+// P.osst.
 __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ctot) {
-    extern __shared__ double s_res[];  // RES: [OV_N][OLF_SEG]
     __shared__ double s_ab[2];
     __shared__ int s_go;
     const int S = P.nseg;
@@ -219,7 +328,6 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ct
     double *const mbuf0 = P.olf_p0, *const mbuf1 = P.olf_p1;
     double *part = P.olf_part;
     double *bbp = P.olf_part + (size_t)6 * S;
-    auto sv = [&](int v, int t) -> double & { return s_res[v * OLF_SEG + t]; };
 
     // ---- r = b - A x, u = r/diag (into m buffer 0), ||b||^2 partials
     for (int s = s_lo; s < s_hi; ++s) {
@@ -234,21 +342,13 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ct
             const double bI = P.olf_b[q.c];
             v[0] += bI * bI;
             double r = 0.0, u = 0.0;
-            const double xc = P.H[q.c];
-            OlfCoef cf{0, 0, 0, 0, 1.0};
             if (!q.ring) {
-                cf = olf_coef(P, D, q.c, ctot);
-                r = bI - olf_av<false>(cf, P.H, q.c, q.nx, xc);
+                const OlfCoef cf = olf_coef(P, D, q.c, ctot);
+                r = bI - olf_av<false>(cf, P.H, q.c, q.nx, P.H[q.c]);
                 u = r / cf.dg;
             }
             mbuf0[q.c] = u;
-            if (RES) {
-                sv(OV_X, t) = xc; sv(OV_R, t) = r;
-                sv(OV_CW, t) = cf.cw; sv(OV_CE, t) = cf.ce; sv(OV_CS, t) = cf.cs; sv(OV_CN, t) = cf.cn;
-                sv(OV_DG, t) = cf.dg;
-            } else {
-                P.olf_r[q.c] = r;
-            }
+            P.olf_r[q.c] = r;
         }
         olf_block_sum<1>(v);
         if (tid == 0) {
@@ -272,10 +372,9 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ct
             if (!q.live) continue;
             double w = 0.0, m = 0.0;
             if (!q.ring) {
-                const OlfCoef cf = RES ? OlfCoef{sv(OV_CW, t), sv(OV_CE, t), sv(OV_CS, t), sv(OV_CN, t), sv(OV_DG, t)}
-                                       : olf_coef(P, D, q.c, ctot);
+                const OlfCoef cf = olf_coef(P, D, q.c, ctot);
                 const double u = __ldcg(mbuf0 + q.c);
-                const double r = RES ? sv(OV_R, t) : P.olf_r[q.c];
+                const double r = P.olf_r[q.c];
                 w = olf_av<true>(cf, mbuf0, q.c, q.nx, u);
                 m = w / cf.dg;
                 v[0] += r * u;
@@ -283,12 +382,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ct
                 v[2] += r * r;
             }
             mbuf1[q.c] = m;
-            if (RES) {
-                sv(OV_W, t) = w;
-                sv(OV_M, t) = m;
-            } else {
-                P.olf_w[q.c] = w;
-            }
+            P.olf_w[q.c] = w;
         }
         olf_block_sum<3>(v);
         if (tid == 0) {
@@ -316,63 +410,29 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ct
             }
             double bbd[1] = {0.0};
             if (it == 0) olf_domain_sum<1>(bbp, S, sg.first, sg.nseg, bbd);
-            bool stopped_now = false;
             if (tid == 0) {
                 OlfSegState st = P.osst[s];
                 if (it == 0) st.bb = bbd[0];
                 int go = 0;
                 if (st.active) {
-                    const double gam = dsum[0], del = dsum[1], rr = dsum[2];
-                    const double tol2 = D.overland_tol * D.overland_tol;
-                    bool stop = rr <= tol2 * st.bb;
-                    stop = stop || it >= D.overland_maxiter || !(rr == rr) || !(gam == gam);
-                    double alpha = 0.0, beta = 0.0;
-                    if (!stop) {
-                        if (it == 0) {
-                            alpha = gam / del;
-                        } else {
-                            beta = gam / st.gamma_prev;
-                            alpha = gam / (del - beta * gam / st.alpha_prev);
-                        }
-                        if (!(alpha > 0.0) || !(alpha < 1e300)) stop = true;  // breakdown
-                    }
-                    if (stop) {
-                        st.active = 0;
-                        stopped_now = true;
-                        if (s == sg.first) {
-                            OverlandCtrl &oc = P.octrl[sg.dom];
-                            oc.iter = it;
-                            oc.rr = rr;
-                            oc.bb = st.bb;
-                        }
-                    } else {
-                        st.gamma_prev = gam;
-                        st.alpha_prev = alpha;
+                    double alpha, beta;
+                    go = olf_decide(P, s, sg, D, it, dsum, st.bb, st.gamma_prev, st.alpha_prev, alpha, beta);
+                    if (go) {
                         st.iter = it + 1;
-                        go = 1;
-                        if (s == sg.first) atomicAdd(&P.gctrl->olf_live[(it + 1) % 3], 1);
                         s_ab[0] = alpha;
                         s_ab[1] = beta;
+                    } else {
+                        st.active = 0;
                     }
                     P.osst[s] = st;
                 }
-                s_go = go | (stopped_now ? 2 : 0);
+                s_go = go;
             }
             __syncthreads();
             const int go = s_go;
             const double alpha = s_ab[0], beta = s_ab[1];
             __syncthreads();
-            if (!(go & 1)) {
-                if (RES && (go & 2)) {
-#pragma unroll
-                    for (int k = 0; k < OLF_CPT; ++k) {
-                        const int t = tid + k * OLF_THREADS;
-                        if (t < sg.count) P.H[sg.begin + t] = sv(OV_X, t);
-                    }
-                }
-                continue;
-            }
-            const bool first = it == 0;
+            if (!go) continue;
             double v[3] = {0.0, 0.0, 0.0};
 #pragma unroll
             for (int k = 0; k < OLF_CPT; ++k) {
@@ -380,40 +440,14 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ct
                 const OlfCell q = olf_cell(sg, D, t);
                 if (!q.live || q.ring) continue;
                 const long long c = q.c;
-                const OlfCoef cf = RES ? OlfCoef{sv(OV_CW, t), sv(OV_CE, t), sv(OV_CS, t), sv(OV_CN, t), sv(OV_DG, t)}
-                                       : olf_coef(P, D, c, ctot);
-                const double mc = RES ? sv(OV_M, t) : __ldcg(mcur + c);
-                const double n = olf_av<true>(cf, mcur, c, q.nx, mc);
-                double r = RES ? sv(OV_R, t) : P.olf_r[c];
-                double w = RES ? sv(OV_W, t) : P.olf_w[c];
-                double x = RES ? sv(OV_X, t) : P.H[c];
-                double z, sdir, p;
-                const double u = r / cf.dg;
-                if (first) {
-                    z = n;
-                    sdir = w;
-                    p = u;
-                } else {
-                    z = n + beta * (RES ? sv(OV_Z, t) : P.olf_z[c]);
-                    sdir = w + beta * (RES ? sv(OV_S, t) : P.olf_s[c]);
-                    p = u + beta * (RES ? sv(OV_P, t) : P.olf_p[c]);
-                }
-                x += alpha * p;
-                r -= alpha * sdir;
-                w -= alpha * z;
-                const double un = r / cf.dg;
-                const double mn = w / cf.dg;
-                v[0] += r * un;
-                v[1] += w * un;
-                v[2] += r * r;
+                const OlfCoef cf = olf_coef(P, D, c, ctot);
+                const double n = olf_av<true>(cf, mcur, c, q.nx, __ldcg(mcur + c));
+                OlfVec e{P.H[c], P.olf_r[c], P.olf_w[c], 0.0, 0.0, 0.0};
+                if (it > 0) { e.z = P.olf_z[c]; e.s = P.olf_s[c]; e.p = P.olf_p[c]; }
+                const double mn = olf_update(e, cf.dg, n, alpha, beta, it == 0, v);
                 mnext[c] = mn;
-                if (RES) {
-                    sv(OV_Z, t) = z; sv(OV_S, t) = sdir; sv(OV_P, t) = p;
-                    sv(OV_X, t) = x; sv(OV_R, t) = r; sv(OV_W, t) = w; sv(OV_M, t) = mn;
-                } else {
-                    P.olf_z[c] = z; P.olf_s[c] = sdir; P.olf_p[c] = p;
-                    P.H[c] = x; P.olf_r[c] = r; P.olf_w[c] = w;
-                }
+                P.olf_z[c] = e.z; P.olf_s[c] = e.s; P.olf_p[c] = e.p;
+                P.H[c] = e.x; P.olf_r[c] = e.r; P.olf_w[c] = e.w;
             }
             olf_block_sum<3>(v);
             if (tid == 0) {
@@ -424,6 +458,176 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ct
         if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
         if (!grid_sync(P.barrier)) return;
         if (__ldcg(&P.gctrl->olf_live[(it + 1) % 3]) == 0) break;
+    }
+}
+
+// Resident variant: one block per segment for the whole solve.  The segment's
+// x, r, w, z, s, p, m and row coefficients stay in shared memory and its CG
+// scalars in thread 0's registers; only m goes through global memory (for the
+// neighbours), and x is written back when the domain stops.  Each iteration
+// is latency-bound, so its global reads -- the domain's partial sums, the
+// neighbour values of m and the liveness count -- are all issued together
+// right after the barrier, and the barrier is a single counter that the
+// blocks add to and poll (olf_sync), with no reset step between iterations.
+__global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long long ctot) {
+    extern __shared__ double s_res[];  // [OV_N][OLF_SEG]
+    __shared__ double s_ab[2];
+    __shared__ int s_go;
+    const int S = P.nseg;
+    const int tid = threadIdx.x;
+    const int s = blockIdx.x;
+    const OlfSeg sg = P.oseg[s];
+    const DomainDesc &D = P.dom[sg.dom];
+    double *const mbuf0 = P.olf_p0, *const mbuf1 = P.olf_p1;
+    double *part = P.olf_part;
+    double *bbp = P.olf_part + (size_t)6 * S;
+    unsigned int *const bar = &P.gctrl->olf_bar;
+    unsigned int epoch = 0;
+    auto sv = [&](int v, int t) -> double & { return s_res[v * OLF_SEG + t]; };
+    auto coef = [&](int t) { return OlfCoef{sv(OV_CW, t), sv(OV_CE, t), sv(OV_CS, t), sv(OV_CN, t), sv(OV_DG, t)}; };
+    OlfCell cell[OLF_CPT];
+#pragma unroll
+    for (int k = 0; k < OLF_CPT; ++k) cell[k] = olf_cell(sg, D, tid + k * OLF_THREADS);
+
+    // ---- r = b - A x, u = r/diag (into m buffer 0), ||b||^2 partials
+    {
+        double v[1] = {0.0};
+#pragma unroll
+        for (int k = 0; k < OLF_CPT; ++k) {
+            const int t = tid + k * OLF_THREADS;
+            const OlfCell &q = cell[k];
+            if (!q.live) continue;
+            const double bI = P.olf_b[q.c];
+            v[0] += bI * bI;
+            double r = 0.0, u = 0.0;
+            const double xc = P.H[q.c];
+            OlfCoef cf{0, 0, 0, 0, 1.0};
+            if (!q.ring) {
+                cf = olf_coef(P, D, q.c, ctot);
+                r = bI - olf_av<false>(cf, P.H, q.c, q.nx, xc);
+                u = r / cf.dg;
+            }
+            mbuf0[q.c] = u;
+            sv(OV_X, t) = xc; sv(OV_R, t) = r;
+            sv(OV_CW, t) = cf.cw; sv(OV_CE, t) = cf.ce; sv(OV_CS, t) = cf.cs; sv(OV_CN, t) = cf.cn;
+            sv(OV_DG, t) = cf.dg;
+        }
+        olf_block_sum<1>(v);
+        if (tid == 0) __stcg(&bbp[s], v[0]);
+    }
+    if (!olf_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
+
+    // ---- w = A u, m_0 = w/diag (into m buffer 1), sums of iteration 0
+    double bb = 0.0;  // the domain's ||b||^2
+    {
+        double bbd[1];
+        olf_domain_sum<1>(bbp, S, sg.first, sg.nseg, bbd);
+        bb = bbd[0];
+        double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < OLF_CPT; ++k) {
+            const int t = tid + k * OLF_THREADS;
+            const OlfCell &q = cell[k];
+            if (!q.live) continue;
+            double w = 0.0, m = 0.0;
+            if (!q.ring) {
+                const OlfCoef cf = coef(t);
+                const double u = __ldcg(mbuf0 + q.c);
+                const double r = sv(OV_R, t);
+                w = olf_av<true>(cf, mbuf0, q.c, q.nx, u);
+                m = w / cf.dg;
+                v[0] += r * u;
+                v[1] += w * u;
+                v[2] += r * r;
+            }
+            mbuf1[q.c] = m;
+            sv(OV_W, t) = w;
+            sv(OV_M, t) = m;
+        }
+        olf_block_sum<3>(v);
+        if (tid == 0) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) __stcg(&part[(size_t)i * S + s], v[i]);
+        }
+    }
+    if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[2] = 0;
+    if (!olf_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
+
+    // ---- iterations
+    bool active = true;                        // this segment's domain still iterates
+    double gamma_prev = 0.0, alpha_prev = 0.0;  // used by thread 0
+    for (int it = 0;; ++it) {
+        const double *pin = part + (size_t)(it & 1) * 3 * S;
+        double *pout = part + (size_t)((it + 1) & 1) * 3 * S;
+        const double *mcur = (it & 1) ? mbuf0 : mbuf1;
+        double *mnext = (it & 1) ? mbuf1 : mbuf0;
+        // every global read of the iteration, issued together
+        const int live = it > 0 ? __ldcg(&P.gctrl->olf_live[it % 3]) : 1;
+        double dpart[3] = {0.0, 0.0, 0.0};
+        for (int k = tid; k < sg.nseg; k += OLF_THREADS) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) dpart[i] += __ldcg(&pin[(size_t)i * S + sg.first + k]);
+        }
+        double nb[OLF_CPT][4];
+#pragma unroll
+        for (int k = 0; k < OLF_CPT; ++k) {
+            const OlfCell &q = cell[k];
+            if (active && q.live && !q.ring) {
+                nb[k][0] = __ldcg(mcur + q.c - 1);
+                nb[k][1] = __ldcg(mcur + q.c + 1);
+                nb[k][2] = __ldcg(mcur + q.c - q.nx);
+                nb[k][3] = __ldcg(mcur + q.c + q.nx);
+            }
+        }
+        if (live == 0) break;  // no domain did work in the previous iteration
+        if (!active) {
+            if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
+            if (!olf_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
+            continue;
+        }
+        olf_block_sum<3>(dpart);
+        if (tid == 0) {
+            double alpha, beta;
+            const int go = olf_decide(P, s, sg, D, it, dpart, bb, gamma_prev, alpha_prev, alpha, beta);
+            s_ab[0] = alpha;
+            s_ab[1] = beta;
+            s_go = go;
+        }
+        __syncthreads();
+        const int go = s_go;
+        const double alpha = s_ab[0], beta = s_ab[1];
+        __syncthreads();
+        if (!go) {
+            active = false;
+#pragma unroll
+            for (int k = 0; k < OLF_CPT; ++k) {
+                const int t = tid + k * OLF_THREADS;
+                if (t < sg.count) P.H[sg.begin + t] = sv(OV_X, t);
+            }
+        } else {
+            double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < OLF_CPT; ++k) {
+                const int t = tid + k * OLF_THREADS;
+                const OlfCell &q = cell[k];
+                if (!q.live || q.ring) continue;
+                const OlfCoef cf = coef(t);
+                const double n = olf_av4(cf, sv(OV_M, t), nb[k][0], nb[k][1], nb[k][2], nb[k][3]);
+                OlfVec e{sv(OV_X, t), sv(OV_R, t), sv(OV_W, t), 0.0, 0.0, 0.0};
+                if (it > 0) { e.z = sv(OV_Z, t); e.s = sv(OV_S, t); e.p = sv(OV_P, t); }
+                const double mn = olf_update(e, cf.dg, n, alpha, beta, it == 0, v);
+                mnext[q.c] = mn;
+                sv(OV_Z, t) = e.z; sv(OV_S, t) = e.s; sv(OV_P, t) = e.p;
+                sv(OV_X, t) = e.x; sv(OV_R, t) = e.r; sv(OV_W, t) = e.w; sv(OV_M, t) = mn;
+            }
+            olf_block_sum<3>(v);
+            if (tid == 0) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) __stcg(&pout[(size_t)i * S + s], v[i]);
+            }
+        }
+        if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
+        if (!olf_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
     }
 }
 
@@ -478,11 +682,11 @@ cudaError_t launch_overland_solve(const DevPtrs &P, const LaunchCfg &L, long lon
     long long c = ctot;
     void *kargs[] = {&args, &c};
     if (L.olf_allow_resident && P.nseg <= L.olf_res_blocks)
-        return cudaLaunchCooperativeKernel((const void *)k_olf_pcg<true>, dim3(P.nseg), dim3(OLF_THREADS), kargs,
+        return cudaLaunchCooperativeKernel((const void *)k_olf_pcg_res, dim3(P.nseg), dim3(OLF_THREADS), kargs,
                                            OLF_RES_SMEM, s);
     const int blocks = L.olf_stream_per_sm * L.sms;
     const int grid = blocks < P.nseg ? blocks : P.nseg;
-    return cudaLaunchCooperativeKernel((const void *)k_olf_pcg<false>, dim3(grid), dim3(OLF_THREADS), kargs, 0, s);
+    return cudaLaunchCooperativeKernel((const void *)k_olf_pcg, dim3(grid), dim3(OLF_THREADS), kargs, 0, s);
 }
 
 cudaError_t launch_overland_finish(const DevPtrs &P, long long ctot, cudaStream_t s) {
@@ -494,15 +698,15 @@ cudaError_t configure_2d(LaunchCfg &L, int device) {
     cudaDeviceProp prop;
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute((const void *)k_olf_pcg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute((const void *)k_olf_pcg_res, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              OLF_RES_SMEM);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_pcg<true>, OLF_THREADS,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_pcg_res, OLF_THREADS,
                                                       OLF_RES_SMEM);
     if (e != cudaSuccess) return e;
     L.olf_res_blocks = per_sm * prop.multiProcessorCount;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_pcg<false>, OLF_THREADS, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_pcg, OLF_THREADS, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     L.olf_stream_blocks = per_sm * prop.multiProcessorCount;
