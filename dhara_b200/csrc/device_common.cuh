@@ -64,6 +64,43 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *gb) {
     return s_ok != 0;
 }
 
+// Grid barrier over a counter: every block adds one (a release reduction)
+// and polls with acquire loads until the count reaches target = epoch x
+// blocks, so no block resets anything between barriers; the count must be
+// zero when the launch starts (the caller zeroes it).  Unlike grid_sync it
+// does not order the phase's writes for TMA reads.  Bounded like grid_sync: a
+// wait beyond BARRIER_TIMEOUT_NS, or an error raised by another block, sets or
+// reads GridBarrier::error and returns false in every thread.
+__device__ __forceinline__ bool counter_sync(unsigned int *count, unsigned int target, GridBarrier *gb) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
+        const unsigned long long t0 = global_ns();
+        unsigned int spins = 0;
+        for (;;) {
+            unsigned int v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+            if ((int)(v - target) >= 0) break;
+            if ((++spins & 63u) == 0) {
+                if (*(volatile int *)&gb->error) {
+                    ok = 0;
+                    break;
+                }
+                if (global_ns() - t0 > BARRIER_TIMEOUT_NS) {
+                    atomicExch(&gb->error, 1);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 // --------------------------------------------------------- reductions
 // Deterministic block sum of NV doubles (fixed warp/shuffle order); the
 // result is returned in every thread.

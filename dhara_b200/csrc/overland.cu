@@ -279,41 +279,6 @@ __device__ __forceinline__ int olf_decide(const DevPtrs &P, int s, const OlfSeg 
     return 1;
 }
 
-// Grid barrier of the resident overland solve: a counter that every block
-// adds one to (a release reduction) and polls until it reaches target =
-// epoch x blocks (acquire loads), so no block has to reset anything between
-// barriers; k_olf_setup zeroes it before each solve.  Bounded like grid_sync:
-// a wait beyond BARRIER_TIMEOUT_NS, or an error raised by another block, sets
-// or reads GridBarrier::error and returns false in every thread.
-__device__ __forceinline__ bool olf_sync(unsigned int *count, unsigned int target, GridBarrier *gb) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
-        const unsigned long long t0 = global_ns();
-        unsigned int spins = 0;
-        for (;;) {
-            unsigned int v;
-            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
-            if ((int)(v - target) >= 0) break;
-            if ((++spins & 63u) == 0) {
-                if (*(volatile int *)&gb->error) {
-                    ok = 0;
-                    break;
-                }
-                if (global_ns() - t0 > BARRIER_TIMEOUT_NS) {
-                    atomicExch(&gb->error, 1);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
 
 // Streaming variant: blocks loop over segments (more segments than resident
 // blocks); the vectors live in global memory and the segment scalars in
@@ -468,7 +433,8 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ct
 // is latency-bound, so its global reads -- the domain's partial sums, the
 // neighbour values of m and the liveness count -- are all issued together
 // right after the barrier, and the barrier is a single counter that the
-// blocks add to and poll (olf_sync), with no reset step between iterations.
+// blocks add to and poll (counter_sync, zeroed by k_olf_setup), with no reset
+// step between iterations.
 __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long long ctot) {
     extern __shared__ double s_res[];  // [OV_N][OLF_SEG]
     __shared__ double s_ab[2];
@@ -515,7 +481,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long lon
         olf_block_sum<1>(v);
         if (tid == 0) __stcg(&bbp[s], v[0]);
     }
-    if (!olf_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
+    if (!counter_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
 
     // ---- w = A u, m_0 = w/diag (into m buffer 1), sums of iteration 0
     double bb = 0.0;  // the domain's ||b||^2
@@ -551,7 +517,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long lon
         }
     }
     if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[2] = 0;
-    if (!olf_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
+    if (!counter_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
 
     // ---- iterations
     bool active = true;                        // this segment's domain still iterates
@@ -582,7 +548,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long lon
         if (live == 0) break;  // no domain did work in the previous iteration
         if (!active) {
             if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
-            if (!olf_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
+            if (!counter_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
             continue;
         }
         olf_block_sum<3>(dpart);
@@ -627,7 +593,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long lon
             }
         }
         if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
-        if (!olf_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
+        if (!counter_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
     }
 }
 
