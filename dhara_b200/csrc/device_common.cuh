@@ -71,11 +71,16 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *gb) {
 // does not order the phase's writes for TMA reads.  Bounded like grid_sync: a
 // wait beyond BARRIER_TIMEOUT_NS, or an error raised by another block, sets or
 // reads GridBarrier::error and returns false in every thread.
-__device__ __forceinline__ bool counter_sync(unsigned int *count, unsigned int target, GridBarrier *gb) {
+// before_arrive() runs in thread 0 after the block's threads have met and
+// before the arrival is released, so what it writes is published with it.
+template <typename BeforeArrive>
+__device__ __forceinline__ bool counter_sync(unsigned int *count, unsigned int target, GridBarrier *gb,
+                                             BeforeArrive before_arrive) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
+        before_arrive();
         asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
         const unsigned long long t0 = global_ns();
         unsigned int spins = 0;
@@ -99,6 +104,10 @@ __device__ __forceinline__ bool counter_sync(unsigned int *count, unsigned int t
     }
     __syncthreads();
     return s_ok != 0;
+}
+
+__device__ __forceinline__ bool counter_sync(unsigned int *count, unsigned int target, GridBarrier *gb) {
+    return counter_sync(count, target, gb, [] {});
 }
 
 // --------------------------------------------------------- reductions

@@ -241,14 +241,10 @@ __device__ __forceinline__ double olf_update(OlfVec &e, double dg, double n, dou
     return e.w / dg;
 }
 
-// Stop test and step lengths of iteration it for segment s (one thread).
-// dsum = the domain's (gamma, delta, r.r).  Returns 1 to iterate, with alpha,
-// beta and the carried gamma_prev, alpha_prev updated, and counts the domain
-// as live for the next iteration; on a stop the domain's first segment
-// records the iteration count and residual.
-__device__ __forceinline__ int olf_decide(const DevPtrs &P, int s, const OlfSeg &sg, const DomainDesc &D, int it,
-                                          const double (&dsum)[3], double bb, double &gamma_prev,
-                                          double &alpha_prev, double &alpha, double &beta) {
+// Stop test and step lengths of iteration it from the domain sums dsum =
+// (gamma, delta, r.r): returns 1 to iterate, with alpha and beta.
+__device__ __forceinline__ int olf_step_lengths(const DomainDesc &D, int it, const double (&dsum)[3], double bb,
+                                                double gamma_prev, double alpha_prev, double &alpha, double &beta) {
     const double gam = dsum[0], del = dsum[1], rr = dsum[2];
     const double tol2 = D.overland_tol * D.overland_tol;
     bool stop = rr <= tol2 * bb;
@@ -264,21 +260,63 @@ __device__ __forceinline__ int olf_decide(const DevPtrs &P, int s, const OlfSeg 
         }
         if (!(alpha > 0.0) || !(alpha < 1e300)) stop = true;  // breakdown
     }
-    if (stop) {
-        if (s == sg.first) {
-            OverlandCtrl &oc = P.octrl[sg.dom];
-            oc.iter = it;
-            oc.rr = rr;
-            oc.bb = bb;
-        }
-        return 0;
-    }
-    gamma_prev = gam;
-    alpha_prev = alpha;
-    if (s == sg.first) atomicAdd(&P.gctrl->olf_live[(it + 1) % 3], 1);
-    return 1;
+    return stop ? 0 : 1;
 }
 
+// The domain-level effects of that decision, by one thread of the domain's
+// first segment: count the domain as live for the next iteration, or record
+// its iteration count and residual when it stops.
+__device__ __forceinline__ void olf_record(const DevPtrs &P, int s, const OlfSeg &sg, int it, int go,
+                                           const double (&dsum)[3], double bb) {
+    if (s != sg.first) return;
+    if (go) {
+        atomicAdd(&P.gctrl->olf_live[(it + 1) % 3], 1);
+    } else {
+        OverlandCtrl &oc = P.octrl[sg.dom];
+        oc.iter = it;
+        oc.rr = dsum[2];
+        oc.bb = bb;
+    }
+}
+
+// Both, for one thread that carries the segment's gamma_prev, alpha_prev.
+__device__ __forceinline__ int olf_decide(const DevPtrs &P, int s, const OlfSeg &sg, const DomainDesc &D, int it,
+                                          const double (&dsum)[3], double bb, double &gamma_prev,
+                                          double &alpha_prev, double &alpha, double &beta) {
+    const int go = olf_step_lengths(D, it, dsum, bb, gamma_prev, alpha_prev, alpha, beta);
+    if (go) {
+        gamma_prev = dsum[0];
+        alpha_prev = alpha;
+    }
+    olf_record(P, s, sg, it, go, dsum, bb);
+    return go;
+}
+
+// Warp sums of NV per-thread values into s_w[i][warp]; after a __syncthreads,
+// olf_sum_warps adds the warp sums in warp order -- the order olf_block_sum
+// uses, so both give the same bits.
+template <int NV>
+__device__ __forceinline__ void olf_warp_partials(const double (&v)[NV], double (*s_w)[OLF_THREADS / 32]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        double a = v[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) s_w[i][warp] = a;
+    }
+}
+
+template <int NV>
+__device__ __forceinline__ void olf_sum_warps(const double (*s_w)[OLF_THREADS / 32], double (&out)[NV]) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        double a = 0.0;
+#pragma unroll
+        for (int w = 0; w < OLF_THREADS / 32; ++w) a += s_w[i][w];
+        out[i] = a;
+    }
+}
 
 // Streaming variant: blocks loop over segments (more segments than resident
 // blocks); the vectors live in global memory and the segment scalars in
@@ -437,8 +475,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg(DevPtrs P, long long ct
 // step between iterations.
 __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long long ctot) {
     extern __shared__ double s_res[];  // [OV_N][OLF_SEG]
-    __shared__ double s_ab[2];
-    __shared__ int s_go;
+    __shared__ double s_wp[3][OLF_THREADS / 32], s_wv[3][OLF_THREADS / 32];
     const int S = P.nseg;
     const int tid = threadIdx.x;
     const int s = blockIdx.x;
@@ -521,7 +558,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long lon
 
     // ---- iterations
     bool active = true;                        // this segment's domain still iterates
-    double gamma_prev = 0.0, alpha_prev = 0.0;  // used by thread 0
+    double gamma_prev = 0.0, alpha_prev = 0.0;
     for (int it = 0;; ++it) {
         const double *pin = part + (size_t)(it & 1) * 3 * S;
         double *pout = part + (size_t)((it + 1) & 1) * 3 * S;
@@ -547,22 +584,24 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long lon
         }
         if (live == 0) break;  // no domain did work in the previous iteration
         if (!active) {
-            if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
-            if (!counter_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
+            if (!counter_sync(bar, (++epoch) * gridDim.x, P.barrier, [&] {
+                    if (blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
+                }))
+                return;
             continue;
         }
-        olf_block_sum<3>(dpart);
-        if (tid == 0) {
-            double alpha, beta;
-            const int go = olf_decide(P, s, sg, D, it, dpart, bb, gamma_prev, alpha_prev, alpha, beta);
-            s_ab[0] = alpha;
-            s_ab[1] = beta;
-            s_go = go;
+        // the domain sums, then every thread takes the same decision from them
+        olf_warp_partials<3>(dpart, s_wp);
+        __syncthreads();
+        double dsum[3];
+        olf_sum_warps<3>(s_wp, dsum);
+        double alpha, beta;
+        const int go = olf_step_lengths(D, it, dsum, bb, gamma_prev, alpha_prev, alpha, beta);
+        if (go) {
+            gamma_prev = dsum[0];
+            alpha_prev = alpha;
         }
-        __syncthreads();
-        const int go = s_go;
-        const double alpha = s_ab[0], beta = s_ab[1];
-        __syncthreads();
+        if (tid == 0) olf_record(P, s, sg, it, go, dsum, bb);
         if (!go) {
             active = false;
 #pragma unroll
@@ -586,14 +625,19 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_pcg_res(DevPtrs P, long lon
                 sv(OV_Z, t) = e.z; sv(OV_S, t) = e.s; sv(OV_P, t) = e.p;
                 sv(OV_X, t) = e.x; sv(OV_R, t) = e.r; sv(OV_W, t) = e.w; sv(OV_M, t) = mn;
             }
-            olf_block_sum<3>(v);
-            if (tid == 0) {
-#pragma unroll
-                for (int i = 0; i < 3; ++i) __stcg(&pout[(size_t)i * S + s], v[i]);
-            }
+            olf_warp_partials<3>(v, s_wv);
         }
-        if (tid == 0 && blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
-        if (!counter_sync(bar, (++epoch) * gridDim.x, P.barrier)) return;
+        // thread 0 publishes the segment's partial sums as it arrives
+        if (!counter_sync(bar, (++epoch) * gridDim.x, P.barrier, [&] {
+                if (go) {
+                    double ps[3];
+                    olf_sum_warps<3>(s_wv, ps);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) __stcg(&pout[(size_t)i * S + s], ps[i]);
+                }
+                if (blockIdx.x == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
+            }))
+            return;
     }
 }
 
