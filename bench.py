@@ -309,7 +309,7 @@ def run_ours(args, world, rank, local):
     krylov_ms_per_inner = kms / kiters if kiters else None
 
     adjoint = run_adjoint(args, local) if args.adjoint_steps > 0 else None
-    ensemble = run_ensemble(args, local) if args.ensemble_steps > 0 else None
+    ensemble = run_ensemble(args, local, world, rank) if args.ensemble_steps > 0 else None
 
     mass_err = dg["storage_change_cum"] - (dg["top_inflow_cum"] - dg["bottom_outflow_cum"])
     inflow = dg["top_inflow_cum"]
@@ -342,57 +342,42 @@ def run_ours(args, world, rank, local):
 
 
 # -------------------------------------------------------------- ensemble
-def run_ensemble(args, local):
+def run_ensemble(args, local, world=1, rank=0):
     """256 independent domains of uneven size (16x16x20 .. 128x128x40), each
     with its own seeded topography, Ks field, van Genuchten parameters and
     rain, advanced together by one handle: every launch of a step covers all
     domains (the persistent solvers schedule their tiles), and the step is
-    replayed from a CUDA graph.  Timed over the 120-step run after warm-up."""
-    import torch
-    import dhara_b200 as db
+    replayed from a CUDA graph.  Timed over the 120-step run after warm-up.
+    With N ranks the domains are sharded over them (dhara_b200.ensemble: a
+    greedy bin-pack on cell count, nothing exchanged while stepping); the time
+    is the slowest rank's and the value counts every domain (the ensemble is
+    fixed, so this is strong scaling)."""
+    from dhara_b200 import ensemble as ens
     from dhara_b200 import inputs
     nsteps = args.ensemble_steps
     doms = inputs.ensemble(256, nsteps=max(nsteps, 1))
     cells = sum(d.ncells for d in doms)
-
-    def solver():
-        s = db.Solver([d.params for d in doms], device=local)
-        for i, d in enumerate(doms):
-            s.load(d, i)
-        s.prepare()
-        return s
-
-    s = solver()
-    s.step(args.warmup, graph=True)
-    s.synchronize()
-    s.close()
-    s = solver()
-    stream = torch.cuda.ExternalStream(s.stream, device=local)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    s.synchronize()
-    torch.cuda.synchronize()
-    lc0 = s.launch_count()
-    e0.record(stream)
-    s.step(nsteps, graph=True)
-    e1.record(stream)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    launches = s.launch_count() - lc0
+    if args.warmup > 0:
+        ens.run_sharded(doms, args.warmup, rank, world, device=local)
+    barrier(world)
+    ms, launches, diags = ens.run_sharded(doms, nsteps, rank, world, device=local)
+    ms_max = max_over_ranks(ms, world)
     worst_mass = 0.0
     kry_nc = olf_nc = solves = 0
     for i in range(len(doms)):
-        dg = s.diagnostics(i)
+        dg = diags[i]
         inflow = dg["top_inflow_cum"]
         if inflow:
             worst_mass = max(worst_mass, abs(dg["storage_change_cum"] - (inflow - dg["bottom_outflow_cum"])) / inflow)
         kry_nc += dg["krylov_nonconverged"]
         olf_nc += dg["overland_nonconverged"]
         solves += dg["picard_iters_total"]
-    s.close()
     return {"workload": "ensemble_256_domains_16x16x20_to_128x128x40", "domains": len(doms), "cells": cells,
-            "steps": nsteps, "ms_per_step": ms / nsteps, "value": cells * nsteps / (ms / 1e3),
-            "unit": "cell-steps/s", "graph": True, "gpu_launches": launches,
+            "steps": nsteps, "ms_per_step": ms_max / nsteps, "value": cells * nsteps / (ms_max / 1e3),
+            "unit": "cell-steps/s", "graph": True, "ranks": world,
+            "scaling": "strong" if world > 1 else None,
+            "shard_balance": ens.balance([d.ncells for d in doms], world),
+            "gpu_launches": launches, "gpu_launches_note": "this rank's" if world > 1 else None,
             "worst_mass_error_over_inflow": worst_mass, "subsurface_solves": solves,
             "subsurface_solves_at_cap": kry_nc, "overland_solves_at_cap": olf_nc}
 

@@ -43,3 +43,62 @@ def test_replica_throughput_two_ranks():
         assert ms_max == 150.0
         assert abs(value - 2 * 1000 * 10 / 0.150) < 1e-6
         assert mx == 1.0
+
+
+def test_partition_covers_every_domain_once_and_balances():
+    import numpy as np
+    from dhara_b200 import ensemble as ens
+    rng = np.random.default_rng(3)
+    cells = rng.integers(16 * 16 * 20, 128 * 128 * 40, size=256)
+    for nranks in (1, 2, 3, 4, 8):
+        share = ens.partition(cells, nranks)
+        assert len(share) == nranks
+        flat = sorted(i for s in share for i in s)
+        assert flat == list(range(len(cells)))
+        assert all(s == sorted(s) for s in share)
+        loads = [int(sum(cells[i] for i in s)) for s in share]
+        # greedy largest-first: no rank exceeds the mean by more than one domain
+        assert max(loads) <= sum(loads) / nranks + int(cells.max())
+        assert ens.partition(cells, nranks) == share  # deterministic
+    assert ens.balance(cells, 8) < 1.02
+    assert ens.partition([], 2) == [[], []]
+
+
+def _gather_worker(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    from dhara_b200 import ensemble as ens
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        cells = [100 + 7 * (i % 13) for i in range(40)]
+        mine = ens.partition(cells, world)[rank]
+        local = {i: {"domain": i, "rank": rank, "picard_iters_total": 10 * i} for i in mine}
+        merged = ens.gather_diagnostics(local, world)
+        q.put((rank, sorted(merged), {i: merged[i]["rank"] for i in merged},
+               sum(merged[i]["picard_iters_total"] for i in merged)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_ensemble_gathers_every_domain_two_ranks():
+    """The host side of the sharded ensemble with world_size 2 on gloo: each
+    rank reports the diagnostics of its own share and every rank ends with
+    all domains', each from the rank the partition gave it to."""
+    from dhara_b200 import ensemble as ens
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gather_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    res = sorted(q.get(timeout=10) for _ in range(world))
+    cells = [100 + 7 * (i % 13) for i in range(40)]
+    owner = {i: r for r, s in enumerate(ens.partition(cells, world)) for i in s}
+    for rank, keys, ranks, total in res:
+        assert keys == list(range(40))
+        assert ranks == owner
+        assert total == 10 * sum(range(40))

@@ -87,3 +87,31 @@ def test_ensemble_256_domains():
         check_domain(st, dg)
         for k in FIELDS:
             assert np.array_equal(st[k], st2[k]), k
+
+
+def test_ensemble_shards_equal_one_handle():
+    """The ensemble split as two ranks would split it (dhara_b200.ensemble),
+    each share advanced by its own handle one after the other on this GPU:
+    every domain ends bit for bit where the single 256-domain handle puts it,
+    so sharding over GPUs changes nothing but the time."""
+    from dhara_b200 import ensemble as ens
+    doms = inputs.ensemble(256, nsteps=2)
+
+    def advance_share(idx):
+        with db.Solver([doms[i].params for i in idx]) as s:
+            for j, i in enumerate(idx):
+                s.load(doms[i], j)
+            s.prepare()
+            s.step(2, graph=True)
+            s.synchronize()
+            return {i: ({k: s.download(k, j) for k in FIELDS}, s.diagnostics(j)) for j, i in enumerate(idx)}
+
+    whole = advance_share(list(range(len(doms))))
+    shares = ens.partition([d.ncells for d in doms], 2)
+    assert ens.balance([d.ncells for d in doms], 2) < 1.01
+    for share in shares:
+        part = advance_share(share)
+        for i, (st, dg) in part.items():
+            for k in FIELDS:
+                assert np.array_equal(st[k], whole[i][0][k]), (i, k)
+            assert dg["krylov_iters_total"] == whole[i][1]["krylov_iters_total"], i
