@@ -78,6 +78,9 @@ def lib():
         "dhara_params_from_config": (ct.c_int, [ct.c_char_p, ct.c_int, ct.c_int, ct.c_int, P(Params),
                                                 P(_abi.ConfigBC)]),
         "dhara_apply_boundary_config": (ct.c_int, [vp, ct.c_int, P(_abi.ConfigBC)]),
+        "dhara_checkpoint_size": (ct.c_int, [vp, i64p]),
+        "dhara_checkpoint": (ct.c_int, [vp, vp, ct.c_int64]),
+        "dhara_restore": (ct.c_int, [vp, vp, ct.c_int64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -297,6 +300,21 @@ class Solver:
             return loss.value, g[0], g[1], g[2]
         _check(lib().dhara_adjoint(self.h, ct.byref(d), ct.byref(loss), None, None, None))
         return loss.value
+
+    def checkpoint(self):
+        """The state a step starts from, for every domain, as a host byte
+        array (dhara_checkpoint); restore() puts it back."""
+        n = ct.c_int64()
+        _check(lib().dhara_checkpoint_size(self.h, ct.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        _check(lib().dhara_checkpoint(self.h, buf.ctypes.data_as(ct.c_void_p), buf.size))
+        return buf
+
+    def restore(self, buf):
+        """Restores a checkpoint() of a handle with the same domains, after
+        this handle's inputs were loaded and prepare() was called."""
+        b = np.ascontiguousarray(buf, dtype=np.uint8)
+        _check(lib().dhara_restore(self.h, b.ctypes.data_as(ct.c_void_p), b.size))
 
     def krylov_traffic(self):
         b = ct.c_double()

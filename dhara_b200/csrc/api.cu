@@ -1625,3 +1625,127 @@ int dhara_autotune(dhara_handle *h, int trial_steps, dhara_launch_config *chosen
     }
     return DHARA_OK;
 }
+
+// ---------------------------------------------------------- checkpoint
+namespace {
+
+// Header of a checkpoint buffer; the arrays follow it in this order:
+// psi^n, theta^n (Ntot doubles each, the handle's pitched layout), top-layer
+// K, ponded depth, overland depth, overland elevation (Ctot doubles each),
+// then ndom PicardCtrl and ndom DevDiag records.
+struct CkptHeader {
+    char magic[8];
+    int32_t version, ndom;
+    int64_t ntot, ctot;
+    int32_t pctrl_bytes, diag_bytes;
+};
+constexpr int32_t CKPT_VERSION = 1;
+constexpr int CKPT_DIM_INTS = 3;  // nx, ny, nz per domain, after the header
+
+size_t ckpt_bytes(const dhara_handle *h) {
+    return sizeof(CkptHeader) + (size_t)h->ndom * CKPT_DIM_INTS * sizeof(int32_t) +
+           ((size_t)2 * h->Ntot + (size_t)4 * h->Ctot) * sizeof(double) +
+           (size_t)h->ndom * (sizeof(PicardCtrl) + sizeof(DevDiag));
+}
+
+// The device arrays of the checkpoint, in buffer order, with their lengths.
+void ckpt_arrays(const dhara_handle *h, double *(&arr)[6], size_t (&len)[6]) {
+    const DevPtrs &P = h->P;
+    double *a[6] = {P.psin, P.thetan, P.ktop, P.ph, P.h, P.H};
+    for (int i = 0; i < 6; ++i) {
+        arr[i] = a[i];
+        len[i] = (size_t)(i < 2 ? h->Ntot : h->Ctot);
+    }
+}
+
+}  // namespace
+
+int dhara_checkpoint_size(dhara_handle *h, int64_t *bytes) {
+    if (!h || !bytes) return fail(DHARA_ERR_INVALID, "NULL argument");
+    *bytes = (int64_t)ckpt_bytes(h);
+    return DHARA_OK;
+}
+
+int dhara_checkpoint(dhara_handle *h, void *buf, int64_t bytes) {
+    if (!h || !buf) return fail(DHARA_ERR_INVALID, "NULL argument");
+    if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
+    if (bytes < (int64_t)ckpt_bytes(h))
+        return fail(DHARA_ERR_INVALID, "checkpoint buffer of %lld bytes is smaller than %lld", (long long)bytes,
+                    (long long)ckpt_bytes(h));
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    unsigned char *q = (unsigned char *)buf;
+    CkptHeader hd{};
+    std::memcpy(hd.magic, "DHARACK", 8);
+    hd.version = CKPT_VERSION;
+    hd.ndom = h->ndom;
+    hd.ntot = h->Ntot;
+    hd.ctot = h->Ctot;
+    hd.pctrl_bytes = (int32_t)sizeof(PicardCtrl);
+    hd.diag_bytes = (int32_t)sizeof(DevDiag);
+    std::memcpy(q, &hd, sizeof(hd));
+    q += sizeof(hd);
+    for (int d = 0; d < h->ndom; ++d) {
+        const int32_t dims[CKPT_DIM_INTS] = {h->hdom[d].nx, h->hdom[d].ny, h->hdom[d].nz};
+        std::memcpy(q, dims, sizeof(dims));
+        q += sizeof(dims);
+    }
+    double *arr[6];
+    size_t len[6];
+    ckpt_arrays(h, arr, len);
+    cudaStream_t s = h->stream;
+    for (int i = 0; i < 6; ++i) {
+        CK(cudaMemcpyAsync(q, arr[i], len[i] * sizeof(double), cudaMemcpyDeviceToHost, s));
+        q += len[i] * sizeof(double);
+    }
+    CK(cudaMemcpyAsync(q, h->P.pctrl, h->ndom * sizeof(PicardCtrl), cudaMemcpyDeviceToHost, s));
+    q += h->ndom * sizeof(PicardCtrl);
+    CK(cudaMemcpyAsync(q, h->P.diag, h->ndom * sizeof(DevDiag), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return check_device_error(h);
+}
+
+int dhara_restore(dhara_handle *h, const void *buf, int64_t bytes) {
+    if (!h || !buf) return fail(DHARA_ERR_INVALID, "NULL argument");
+    if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
+    if (bytes < (int64_t)sizeof(CkptHeader)) return fail(DHARA_ERR_INVALID, "checkpoint buffer too small");
+    const unsigned char *q = (const unsigned char *)buf;
+    CkptHeader hd;
+    std::memcpy(&hd, q, sizeof(hd));
+    if (std::memcmp(hd.magic, "DHARACK", 8) != 0 || hd.version != CKPT_VERSION)
+        return fail(DHARA_ERR_INVALID, "not a checkpoint of this library version");
+    if (hd.ndom != h->ndom || hd.ntot != h->Ntot || hd.ctot != h->Ctot ||
+        hd.pctrl_bytes != (int32_t)sizeof(PicardCtrl) || hd.diag_bytes != (int32_t)sizeof(DevDiag))
+        return fail(DHARA_ERR_INVALID, "checkpoint of %d domains / %lld cells does not match this handle "
+                    "(%d / %lld)", hd.ndom, (long long)hd.ntot, h->ndom, (long long)h->Ntot);
+    if (bytes < (int64_t)ckpt_bytes(h))
+        return fail(DHARA_ERR_INVALID, "checkpoint buffer of %lld bytes is smaller than %lld", (long long)bytes,
+                    (long long)ckpt_bytes(h));
+    q += sizeof(hd);
+    for (int d = 0; d < h->ndom; ++d) {
+        int32_t dims[CKPT_DIM_INTS];
+        std::memcpy(dims, q, sizeof(dims));
+        q += sizeof(dims);
+        if (dims[0] != h->hdom[d].nx || dims[1] != h->hdom[d].ny || dims[2] != h->hdom[d].nz)
+            return fail(DHARA_ERR_INVALID, "checkpoint domain %d is %dx%dx%d, the handle's is %dx%dx%d", d,
+                        dims[0], dims[1], dims[2], h->hdom[d].nx, h->hdom[d].ny, h->hdom[d].nz);
+    }
+    if (set_dev(h)) return DHARA_ERR_CUDA;
+    double *arr[6];
+    size_t len[6];
+    ckpt_arrays(h, arr, len);
+    cudaStream_t s = h->stream;
+    const DevPtrs &P = h->P;
+    for (int i = 0; i < 6; ++i) {
+        CK(cudaMemcpyAsync(arr[i], q, len[i] * sizeof(double), cudaMemcpyHostToDevice, s));
+        q += len[i] * sizeof(double);
+    }
+    // the Krylov warm start and the Picard iterate of a step's first
+    // iteration are psi^n
+    CK(cudaMemcpyAsync(P.x, P.psin, (size_t)h->Ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.psim, P.psin, (size_t)h->Ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(P.pctrl, q, h->ndom * sizeof(PicardCtrl), cudaMemcpyHostToDevice, s));
+    q += h->ndom * sizeof(PicardCtrl);
+    CK(cudaMemcpyAsync(P.diag, q, h->ndom * sizeof(DevDiag), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return DHARA_OK;
+}

@@ -297,6 +297,24 @@ int dhara_snapshot(dhara_handle *h, int domain, double *water_elevation, double 
                    double *pressure_head, double *moisture);
 int dhara_snapshot_wait(dhara_handle *h);
 
+/* ---- checkpoint and restart -------------------------------------------------
+ * The reference has no restart path (it runs one time loop from the initial
+ * condition, src/device.cu:374-475); these save and restore the state a step
+ * starts from, for every domain of the handle: psi^n, theta^n, the top
+ * layer's K, the ponded depth, the overland depth and elevation, the Picard
+ * control record (step counter, last iteration counts) and the cumulative
+ * diagnostics.  Inputs that do not change during a run (soil and surface
+ * fields, boundary conditions, rain schedule, roots) are not part of it: a
+ * restart uploads them as the original run did, calls dhara_prepare, then
+ * dhara_restore, and its steps then match the original handle's bit for bit.
+ * The buffer is host memory the caller owns; the layout is private to this
+ * library version (a header records the domain sizes, and a checkpoint from
+ * a handle with other domains is rejected with DHARA_ERR_INVALID).  Both
+ * calls synchronise the handle's stream and need dhara_prepare first. */
+int dhara_checkpoint_size(dhara_handle *h, int64_t *bytes);
+int dhara_checkpoint(dhara_handle *h, void *buf, int64_t bytes);
+int dhara_restore(dhara_handle *h, const void *buf, int64_t bytes);
+
 /* ---- configuration file ----------------------------------------------------
  * The reference's "KEY = value" configuration file (parsed by
  * ParserConfigFile, src/parser.cc:39-72; keys read by LoadFlowModelConfig,
