@@ -81,6 +81,7 @@ def lib():
         "dhara_checkpoint_size": (ct.c_int, [vp, i64p]),
         "dhara_checkpoint": (ct.c_int, [vp, vp, ct.c_int64]),
         "dhara_restore": (ct.c_int, [vp, vp, ct.c_int64]),
+        "dhara_selftest_bounded_wait": (ct.c_int, [ct.c_int, ct.c_double, P(ct.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -321,6 +322,14 @@ class Solver:
         n = ct.c_int64()
         _check(lib().dhara_get_krylov_traffic(self.h, ct.byref(b), ct.byref(n)))
         return b.value, n.value
+
+
+def selftest_bounded_wait(limit_ms=200.0, device=0):
+    """Runs a device-side wait that nothing satisfies (dhara_selftest_bounded_wait);
+    True when it gave up after limit_ms, flagged the error and returned."""
+    out = ct.c_int(0)
+    _check(lib().dhara_selftest_bounded_wait(device, float(limit_ms), ct.byref(out)))
+    return bool(out.value)
 
 
 def run(domains, nsteps=None, graph=False, record=(), device=0):

@@ -75,7 +75,8 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *gb) {
 // before the arrival is released, so what it writes is published with it.
 template <typename BeforeArrive>
 __device__ __forceinline__ bool counter_sync(unsigned int *count, unsigned int target, GridBarrier *gb,
-                                             BeforeArrive before_arrive) {
+                                             BeforeArrive before_arrive,
+                                             unsigned long long limit_ns = BARRIER_TIMEOUT_NS) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -93,7 +94,7 @@ __device__ __forceinline__ bool counter_sync(unsigned int *count, unsigned int t
                     ok = 0;
                     break;
                 }
-                if (global_ns() - t0 > BARRIER_TIMEOUT_NS) {
+                if (global_ns() - t0 > limit_ns) {
                     atomicExch(&gb->error, 1);
                     ok = 0;
                     break;

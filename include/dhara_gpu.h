@@ -311,6 +311,16 @@ int dhara_snapshot_wait(dhara_handle *h);
  * library version (a header records the domain sizes, and a checkpoint from
  * a handle with other domains is rejected with DHARA_ERR_INVALID).  Both
  * calls synchronise the handle's stream and need dhara_prepare first. */
+/* ---- failure detection self-check ---------------------------------------------
+ * No counterpart in the reference (which exits on any CUDA error).  Every
+ * device-side wait of the persistent solvers (grid barriers, TMA stage
+ * waits) is bounded: past its limit the kernel raises an error flag and
+ * returns, and the host reports DHARA_ERR_TIMEOUT instead of hanging.  This
+ * runs one such wait on `device` that nothing can satisfy, with the given
+ * limit (0 < limit_ms <= 10000), and sets *timed_out = 1 when the wait gave
+ * up, flagged the error and returned and the context still worked after. */
+int dhara_selftest_bounded_wait(int device, double limit_ms, int *timed_out);
+
 int dhara_checkpoint_size(dhara_handle *h, int64_t *bytes);
 int dhara_checkpoint(dhara_handle *h, void *buf, int64_t bytes);
 int dhara_restore(dhara_handle *h, const void *buf, int64_t bytes);

@@ -1,7 +1,8 @@
 """Checkpoint and restart (dhara_checkpoint / dhara_restore): a handle rebuilt
 from the same inputs and restored from a checkpoint continues exactly where
 the original handle was, bit for bit, for every domain; a checkpoint of other
-domains, or bytes that are not a checkpoint, are rejected."""
+domains, or bytes that are not a checkpoint, are rejected.  And the failure
+detection under them: a bounded device-side wait gives up and reports."""
 import numpy as np
 import pytest
 
@@ -64,3 +65,18 @@ def test_restore_rejects_other_domains_and_garbage():
             b.restore(np.zeros(64, np.uint8))
         with pytest.raises(db.DharaError):
             b.restore(ck[:100])
+
+
+def test_bounded_wait_gives_up_and_context_survives():
+    """Failure detection without a fault: a device-side wait that nothing can
+    satisfy gives up after its 200 ms limit, flags the error and returns; the
+    same process then runs a solver normally."""
+    import time
+    t0 = time.perf_counter()
+    assert db.selftest_bounded_wait(200.0)
+    assert 0.2 <= time.perf_counter() - t0 < 10.0
+    doms = domains()
+    with fresh(doms) as s:
+        s.step(1)
+        s.synchronize()
+        assert s.diagnostics(0)["nonfinite"] == 0
