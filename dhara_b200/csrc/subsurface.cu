@@ -851,23 +851,46 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 3) k_krylov
         if (!grid_sync(P.barrier)) return;
         if (ldcg(&P.gctrl->n_active) == 0) break;
         // ---- inner PCG
+        // A domain's control record (inner_active, parity, first_inner, alpha,
+        // beta) changes only when its last tile of a phase finishes, after
+        // every tile of it in that phase has been scheduled, so within a phase
+        // a block reads it once per domain rather than once per tile.
+        struct Ctl {
+            int dom, active, parity;
+            bool first;
+            double ab;  // beta in phase A, alpha in phase B
+        };
+        auto ctl_load = [&](Ctl &c, int dom, bool phase_a) {
+            if (c.dom == dom) return;
+            const KrylovCtrl *k = &P.kctrl[dom];
+            c.dom = dom;
+            c.active = ldcg(&k->inner_active);
+            c.parity = ldcg(&k->parity);
+            c.first = ldcg(&k->first_inner) != 0;
+            c.ab = phase_a ? ldcg(&k->beta) : ldcg(&k->alpha);
+        };
+        // next tile of this block (stride gridDim.x) whose domain iterates
+        auto next_live = [&](Ctl &c, int t, bool phase_a) {
+            for (; t < P.ntiles; t += gridDim.x) {
+                const int dom = P.tiles[t].dom;
+                if (dom != c.dom) ctl_load(c, dom, phase_a);
+                if (c.active) break;
+            }
+            return t;
+        };
         while (ldcg(&P.gctrl->n_inner_active) > 0) {
             bool pre = false;
-            for (int t = next_inner(blockIdx.x); t < P.ntiles;) {
-                const int tn = next_inner(t + gridDim.x);
+            Ctl cc{-1, 0, 0, false, 0.0}, cn{-1, 0, 0, false, 0.0};
+            for (int t = next_live(cc, blockIdx.x, true); t < P.ntiles;) {
+                const int tn = next_live(cn, t + gridDim.x, true);
                 const int dom = P.tiles[t].dom;
-                const KrylovCtrl *kc = &P.kctrl[dom];
+                ctl_load(cc, dom, true);
                 const ColumnRef cr = column_of(P, t);
-                const int parity = ldcg(&kc->parity);
-                const bool first = ldcg(&kc->first_inner) != 0;
-                const T beta = (T)ldcg(&kc->beta);
-                bool first_n = false;
-                int parity_n = 0;
-                if (tn < P.ntiles) {
-                    const KrylovCtrl *kn = &P.kctrl[P.tiles[tn].dom];
-                    first_n = ldcg(&kn->first_inner) != 0;
-                    parity_n = ldcg(&kn->parity);
-                }
+                const int parity = cc.parity;
+                const bool first = cc.first;
+                const T beta = (T)cc.ab;
+                const bool first_n = tn < P.ntiles ? cn.first : false;
+                const int parity_n = tn < P.ntiles ? cn.parity : 0;
                 T *pnew = (T *)(parity ? P.p0 : P.p1);
                 double v[1] = {0.0};
                 phase_A<T>(P, t, tn, pre, first_n, parity_n, cr, weights(dom), beta, first, parity, pnew,
@@ -884,22 +907,19 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 3) k_krylov
             }
             if (!grid_sync(P.barrier)) return;
             pre = false;
-            for (int t = next_inner(blockIdx.x); t < P.ntiles;) {
-                const int tn = next_inner(t + gridDim.x);
+            cc = Ctl{-1, 0, 0, false, 0.0};
+            cn = Ctl{-1, 0, 0, false, 0.0};
+            for (int t = next_live(cc, blockIdx.x, false); t < P.ntiles;) {
+                const int tn = next_live(cn, t + gridDim.x, false);
                 const int dom = P.tiles[t].dom;
-                const KrylovCtrl *kc = &P.kctrl[dom];
+                ctl_load(cc, dom, false);
                 const ColumnRef cr = column_of(P, t);
                 const DomainDesc &D = P.dom[dom];
-                const int parity = ldcg(&kc->parity);
-                const bool first = ldcg(&kc->first_inner) != 0;
-                const T alpha = (T)ldcg(&kc->alpha);
-                bool first_n = false;
-                int parity_n = 0;
-                if (tn < P.ntiles) {
-                    const KrylovCtrl *kn = &P.kctrl[P.tiles[tn].dom];
-                    first_n = ldcg(&kn->first_inner) != 0;
-                    parity_n = ldcg(&kn->parity);
-                }
+                const int parity = cc.parity;
+                const bool first = cc.first;
+                const T alpha = (T)cc.ab;
+                const bool first_n = tn < P.ntiles ? cn.first : false;
+                const int parity_n = tn < P.ntiles ? cn.parity : 0;
                 double v[2] = {0.0, 0.0};
                 phase_B<T, DSMEM>(P, t, tn, pre, first_n, parity_n, cr, alpha, first, parity, s_d, stage_raw,
                                   sb, v);
