@@ -329,6 +329,8 @@ def run_ours(args, world, rank, local):
         "picard_iters": dg["picard_iters_total"], "krylov_inner_iters": dg["krylov_iters_total"],
         "refine_cycles": dg["refine_iters_total"], "overland_iters": dg["overland_iters_total"],
         "krylov_ms_per_inner_iter": krylov_ms_per_inner,
+        "krylov_solves_at_cap": dg["krylov_nonconverged"], "overland_solves_at_cap": dg["overland_nonconverged"],
+        "picard_steps_at_cap": dg["picard_nonconverged"],
         "adjoint_over_forward": adjoint["adjoint_over_forward"] if adjoint else None,
         "adjoint": adjoint,
         "ensemble": ensemble,
