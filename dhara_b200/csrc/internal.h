@@ -64,8 +64,8 @@ struct KrylovCtrl {
     double bb;          // ||b||^2 of the 3D system
     double rr64;        // ||b - A x||^2 at the last outer check
     double rr;          // inner residual^2
-    double rz, rz_old;  // preconditioned inner products
-    double pAp, alpha, beta;
+    double rz;          // preconditioned inner product r.z
+    double alpha, beta;
     double inner_target2;
     int active;         // outer solve still running
     int inner_active;   // inner PCG running
@@ -86,8 +86,8 @@ struct PicardCtrl {
 };
 
 struct OverlandCtrl {
-    double bb, rr, rz, rz_old, pAp, alpha, beta;
-    int active, iter, parity, pad;
+    double bb, rr;  // ||b||^2 and the final ||r||^2 of the domain's last solve
+    int iter, pad;  // its iteration count
 };
 
 // The overland solve works on segments: up to OLF_SEG consecutive surface

@@ -898,7 +898,6 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 3) k_krylov
                 pre = tn < P.ntiles;
                 if (domain_reduce<1>(P, t, dom, 0, v) && threadIdx.x == 0) {
                     KrylovCtrl &c = P.kctrl[dom];
-                    c.pAp = v[0];
                     c.alpha = c.rz / v[0];
                     c.parity ^= 1;
                     if (!(v[0] > 0.0) || isinf(v[0])) stop_inner(P, c);
