@@ -150,7 +150,7 @@ struct DevPtrs {
     const DomainDesc *dom;
     const TileDesc *tiles;
     int ntiles, ndom;
-    int smem_nz;         // column capacity of the Thomas buffers in shared memory
+    int smem_nz;         // column capacity of the d' buffer of the column solves in shared memory
     int pad_smem;
     // 3D double state
     double *psin, *thetan, *psim, *x, *b, *ksat, *alpha, *nvg;

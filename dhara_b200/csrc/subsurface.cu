@@ -725,7 +725,7 @@ __device__ void phase_A(const DevPtrs &P, int tile, int tile_next, bool prefetch
 
 // ---- phase B: update, residual, preconditioner --------------------------------
 // d += alpha p, r -= alpha q, z = M^-1 r with the stored factors;
-// v = {||r||^2, r.z}.  Column-local: staged p, q, d, r, 1/den, a/den (own).
+// v = {||r||^2, r.z}.  Column-local: staged p, q, d, r, 1/den, c' (own).
 template <typename T, bool DSMEM>
 __device__ void phase_B(const DevPtrs &P, int tile, int tile_next, bool prefetched, bool first_next,
                         int parity_next, const ColumnRef &cr, T alpha, bool first, int parity_p, T *s_d,
