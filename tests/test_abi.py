@@ -86,6 +86,21 @@ def test_null_arguments():
     assert L.dhara_create(None, 1, 0, None) == 1
     assert L.dhara_step(None, 1, 0) == 1
     assert L.dhara_destroy(None) == 0
+    n = ct.c_int64(-1)
+    assert L.dhara_checkpoint_size(None, ct.byref(n)) == 1
+    assert L.dhara_checkpoint(None, None, 0) == 1
+    assert L.dhara_restore(None, None, 0) == 1
+
+
+def test_bounded_wait_selftest_validates_before_touching_the_gpu():
+    """The self-check's limit is validated on the host: out-of-range limits
+    and a NULL result pointer are rejected without a device."""
+    L = db.lib()
+    out = ct.c_int(7)
+    for bad in (0.0, -1.0, 1e9, float("nan")):
+        assert L.dhara_selftest_bounded_wait(0, bad, ct.byref(out)) == 1
+        assert b"limit_ms" in L.dhara_last_error()
+    assert L.dhara_selftest_bounded_wait(0, 100.0, None) == 1
 
 
 def test_oracle_library_loads():
