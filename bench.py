@@ -557,8 +557,10 @@ def run_reference(args, world, rank):
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": done,
             "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(done, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"mixed_{args.nx}x{args.nx}x{args.nz} (CPU patch "
-                                   f"{d.params.nx}x{d.params.ny}x{d.params.nz})"},
+            "config": {"workload": f"mixed_{args.nx}x{args.nx}x{args.nz}",
+                       "cells": args.nx * args.nx * args.nz,
+                       "cpu_patch": f"{d.params.nx}x{d.params.ny}x{d.params.nz}",
+                       "precision": "fp64 (the reference's)", "parallelism": f"{threads} host threads"},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
