@@ -102,3 +102,20 @@ def test_sharded_ensemble_gathers_every_domain_two_ranks():
         assert keys == list(range(40))
         assert ranks == owner
         assert total == 10 * sum(range(40))
+
+
+def test_partition_of_the_benchmark_ensemble():
+    """The 256-domain ensemble of the benchmark splits evenly enough that the
+    slowest rank's share is within 1 % (2 ranks) and 3 % (8 ranks) of the mean."""
+    import numpy as np
+    from dhara_b200 import ensemble as ens
+    rng = np.random.default_rng(3)   # the draws of inputs.ensemble(256, seed=3), sizes only
+    cells = []
+    for _ in range(256):
+        nx, ny, nz = (int(rng.integers(16, 129)), int(rng.integers(16, 129)), int(rng.integers(20, 41)))
+        rng.integers(0, 2**31 - 1); rng.uniform(0.5, 1.5); rng.uniform(1.0, 5.0); rng.uniform(1.3, 2.2)
+        rng.uniform(5.0, 40.0)
+        cells.append(nx * ny * nz)
+    assert sum(cells) == 42384095  # the ensemble's cell count in the benchmark line
+    assert ens.balance(cells, 2) < 1.01
+    assert ens.balance(cells, 8) < 1.03
