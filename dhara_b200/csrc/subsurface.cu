@@ -804,7 +804,7 @@ __device__ __forceinline__ void stop_inner(const DevPtrs &P, KrylovCtrl &c) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 3) k_krylov(DevPtrs P) {
+__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 4) k_krylov(DevPtrs P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar[STAGES];
     constexpr bool DSMEM = sizeof(T) == 4;
