@@ -20,7 +20,7 @@
 #define NZ_MAX 64
 // planes per TMA-staged chunk: inner phases (by inner precision) and the FP64 residual
 #define CHUNK_F32 3
-#define CHUNK_F64 2
+#define CHUNK_F64 4
 #define CH_R 2
 // TMA staging buffers per block (chunks in flight ahead of the one being computed: STAGES - 1)
 #define STAGES 2
