@@ -31,22 +31,34 @@ def stale():
     return any(os.path.getmtime(f) > t for f in SRC + HDRS)
 
 
-def build(force=False, verbose=False, extra=()):
-    if not force and not stale():
+def build(force=False, verbose=False, extra=(), out=None):
+    """Compiles every csrc/*.cu for sm_100a and links the library (to `out`,
+    default dhara_b200/libdhara_b200.so); `extra` adds nvcc flags."""
+    if out is None and not force and not stale():
         return LIB
-    objs = []
+    from concurrent.futures import ThreadPoolExecutor
     bdir = os.path.join(HERE, "_build")
+    if out is not None:
+        bdir = os.path.join(bdir, os.path.splitext(os.path.basename(out))[0])
     os.makedirs(bdir, exist_ok=True)
+    cmds = []
+    objs = []
     for src in SRC:
         obj = os.path.join(bdir, os.path.basename(src) + ".o")
-        cmd = [nvcc(), *NVCC_FLAGS, *extra, "-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
+        cmds.append([nvcc(), *NVCC_FLAGS, *extra, "-c", src, "-o", obj])
         objs.append(obj)
-    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs]
+    if verbose:
+        for cmd in cmds:
+            print(" ".join(cmd), file=sys.stderr)
+    # the translation units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for r in pool.map(lambda c: subprocess.run(c, capture_output=not verbose, text=True), cmds):
+            if r.returncode != 0:
+                sys.stderr.write((r.stdout or "") + (r.stderr or ""))
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", out or LIB, *objs]
     subprocess.run(cmd, check=True)
-    return LIB
+    return out or LIB
 
 
 if __name__ == "__main__":

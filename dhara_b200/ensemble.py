@@ -45,7 +45,8 @@ def run_sharded(domains, nsteps, rank, world, device=0, graph=True):
     """Advances this rank's share of `domains` (inputs.Domain objects) for
     nsteps in one handle on `device`; returns this rank's device time in ms
     (CUDA events on the handle's stream), the number of kernel launches it
-    made, and the diagnostics of all domains, gathered from every rank."""
+    made, and the diagnostics of all domains (plus each domain's largest
+    |psi| after the run, "psi_abs_max"), gathered from every rank."""
     import torch
     import dhara_b200 as db
     cells = [d.ncells for d in domains]
@@ -71,6 +72,7 @@ def run_sharded(domains, nsteps, rank, world, device=0, graph=True):
             launches = s.launch_count() - lc0
             for j, i in enumerate(mine):
                 local[i] = s.diagnostics(j)
+                local[i]["psi_abs_max"] = float(np.abs(s.download("psi", j)).max())
         finally:
             s.close()
     return ms, launches, gather_diagnostics(local, world)

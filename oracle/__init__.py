@@ -14,7 +14,7 @@ from dhara_b200 import _abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
-SOLVER_BICGSTAB, SOLVER_CG = 0, 1
+SOLVER_BICGSTAB, SOLVER_CG, SOLVER_PCG_COLUMN = 0, 1, 2
 
 _lib = None
 

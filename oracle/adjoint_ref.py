@@ -22,10 +22,100 @@ faces, in metres summed over cells).
 """
 import numpy as np
 import torch
+import torch.nn.functional as F
 
 from dhara_b200 import _abi
 
 T = torch.float64
+
+
+# ------------------------------------------------------- sparse exact solves
+# For domains too large for dense matrices the linear systems are solved by
+# preconditioned CG to a relative residual of 1e-14 and differentiated
+# implicitly: x = x* + A^-1 (b - A x*) with x* the (detached) solution, whose
+# value is x* and whose derivative is A^-1 (db - dA x*) -- the exact-solve
+# derivative, because A is symmetric the backward pass is another solve with A.
+
+def _pcg(apply, precond, b, x0, tol, maxiter):
+    """Preconditioned CG (no autograd) to ||b - A x|| <= tol ||b||."""
+    x = x0.clone()
+    r = b - apply(x)
+    bn = float(torch.linalg.vector_norm(b))
+    if bn == 0.0:
+        return torch.zeros_like(b)
+    z = precond(r)
+    p = z.clone()
+    rz = torch.sum(r * z)
+    for _ in range(maxiter):
+        if float(torch.linalg.vector_norm(r)) <= tol * bn:
+            break
+        q = apply(p)
+        a = rz / torch.sum(p * q)
+        x = x + a * p
+        r = r - a * q
+        z = precond(r)
+        rz_n = torch.sum(r * z)
+        p = z + (rz_n / rz) * p
+        rz = rz_n
+    else:
+        raise RuntimeError("reference PCG did not reach its tolerance")
+    return x
+
+
+class _ApplyInverse(torch.autograd.Function):
+    """y = A^-1 r for a symmetric positive definite A given as a solver;
+    the backward pass applies the same solver to the incoming gradient."""
+
+    @staticmethod
+    def forward(ctx, r, solver):
+        ctx.solver = solver
+        return solver(r)
+
+    @staticmethod
+    def backward(ctx, g):
+        return ctx.solver(g), None
+
+
+def implicit_solve(matvec, precond, b, x0, tol=1e-14, maxiter=100000):
+    """Solution of A x = b with exact-solve derivatives; matvec(v) = A v is
+    differentiable in A's coefficients, precond(r) ~ A^-1 r (no autograd)."""
+    with torch.no_grad():
+        app = lambda v: matvec(v)
+        xs = _pcg(app, precond, b.detach(), x0.detach(), tol, maxiter)
+    solver = lambda v: _pcg(lambda u: matvec(u).detach(), precond, v.detach(), torch.zeros_like(v), tol, maxiter)
+    return xs + _ApplyInverse.apply(b - matvec(xs), solver)
+
+
+def matvec3(x, Dg, kz, ky, kx):
+    """7-point operator D x + sum_f k_f (x_c - x_f) on a [nz, ny, nx] grid,
+    zero flux through the domain faces (k* are face coefficients / h^2)."""
+    fz = kz * (x[:-1] - x[1:])
+    fy = ky * (x[:, :-1] - x[:, 1:])
+    fx = kx * (x[:, :, :-1] - x[:, :, 1:])
+    return (Dg * x + F.pad(fz, (0, 0, 0, 0, 0, 1)) - F.pad(fz, (0, 0, 0, 0, 1, 0))
+            + F.pad(fy, (0, 0, 0, 1)) - F.pad(fy, (0, 0, 1, 0)) + F.pad(fx, (0, 1)) - F.pad(fx, (1, 0)))
+
+
+def column_preconditioner(Dg, kz, ky, kx):
+    """r -> M^-1 r with M the vertical (k) tridiagonal part of the operator."""
+    with torch.no_grad():
+        dg = (Dg + F.pad(kz, (0, 0, 0, 0, 0, 1)) + F.pad(kz, (0, 0, 0, 0, 1, 0)) + F.pad(ky, (0, 0, 0, 1))
+              + F.pad(ky, (0, 0, 1, 0)) + F.pad(kx, (0, 1)) + F.pad(kx, (1, 0)))
+        off = -kz
+        nz = dg.shape[0]
+        den, cp = [dg[0]], []
+        for k in range(1, nz):
+            cp.append(off[k - 1] / den[k - 1])
+            den.append(dg[k] - off[k - 1] * cp[k - 1])
+
+    def apply(r):
+        y = [r[0] / den[0]]
+        for k in range(1, nz):
+            y.append((r[k] - off[k - 1] * y[k - 1]) / den[k])
+        for k in range(nz - 2, -1, -1):
+            y[k] = y[k] - cp[k] * y[k + 1]
+        return torch.stack(y)
+    return apply
 
 
 def closure(psi, ks, alpha_m, n, ts, tr):
@@ -49,10 +139,16 @@ def closure(psi, ks, alpha_m, n, ts, tr):
 
 
 class Model:
-    """The coupled model on one small domain (reference layouts flattened to
-    [nz, ny, nx] and [ny, nx] grids)."""
+    """The coupled model on one domain (reference layouts flattened to
+    [nz, ny, nx] and [ny, nx] grids).  sparse=False builds the linear systems
+    dense and solves them directly (small domains); sparse=True applies them
+    as stencils and solves them by PCG to 1e-14 with implicit derivatives, and
+    checkpoint=True recomputes each time step in the backward pass instead of
+    keeping its graph (the 128x128x30 calibration domain)."""
 
-    def __init__(self, domain):
+    def __init__(self, domain, sparse=False, checkpoint=False):
+        self.sparse = sparse
+        self.checkpoint = checkpoint
         p = domain.params
         self.p = p
         self.nx, self.ny, self.nz = p.nx, p.ny, p.nz
@@ -111,6 +207,12 @@ class Model:
             A = A.index_put((b, b), kf, accumulate=True)
             A = A.index_put((a, b), -kf, accumulate=True)
             A = A.index_put((b, a), -kf, accumulate=True)
+        return A, self.rhs3(psi_m, psin, thetan, theta_m, K, Cm, qt).reshape(-1)
+
+    def rhs3(self, psi_m, psin, thetan, theta_m, K, Cm, qt):
+        """Right-hand side of SetUpLinearSystemsSubsurface for the scope."""
+        p = self.p
+        nz = self.nz
         # rhs: storage, C psi^m, gravity, theta change
         rhs = (p.Ss / p.dt * theta_m / p.porosity * psin + Cm / p.dt * psi_m + (thetan - theta_m) / p.dt)
         # gravity -(ku - kd)/dz with ku the face below (k+1) and kd the face above (k-1)
@@ -124,8 +226,16 @@ class Model:
         top[0] = qt / p.dz
         bot = torch.zeros_like(K)
         bot[nz - 1] = -K[nz - 1] / p.dz
-        rhs = rhs + top + bot
-        return A, rhs.reshape(-1)
+        return rhs + top + bot
+
+    def coeffs3(self, theta_m, K, Cm):
+        """Storage diagonal and face coefficients (arithmetic-mean K / h^2)."""
+        p = self.p
+        Dg = p.Ss / p.dt * theta_m / p.porosity + Cm / p.dt
+        kz = 0.5 * (K[:-1] + K[1:]) / (p.dz ** 2)
+        ky = 0.5 * (K[:, :-1] + K[:, 1:]) / (p.dy ** 2)
+        kx = 0.5 * (K[:, :, :-1] + K[:, :, 1:]) / (p.dx ** 2)
+        return Dg, kz, ky, kx
 
     def prologue(self, ph, psin_top, K_top, ks_top, thetan_top, rain_mm):
         """EstimateFluxes + IdentifyTopBoundary (src/global.cu:172-257) with
@@ -148,8 +258,15 @@ class Model:
         it = 0
         while True:
             theta_m, K_m, C_m = closure(psi_m, ks, al, nv, p.theta_s, p.theta_r)
-            A, rhs = self.assemble(psi_m, psin, thetan, theta_m, K_m, C_m, qt)
-            x = torch.linalg.solve(A, rhs).reshape(psin.shape)
+            if self.sparse:
+                co = self.coeffs3(theta_m, K_m, C_m)
+                rhs = self.rhs3(psi_m, psin, thetan, theta_m, K_m, C_m, qt)
+                pre = column_preconditioner(*[c.detach() for c in co])
+                # bind this iteration's coefficients (the backward solve runs later)
+                x = implicit_solve(lambda v, co=co: matvec3(v, *co), pre, rhs, psi_m)
+            else:
+                A, rhs = self.assemble(psi_m, psin, thetan, theta_m, K_m, C_m, qt)
+                x = torch.linalg.solve(A, rhs).reshape(psin.shape)
             it += 1
             if p.picard_rule == _abi.PICARD_PSI_ABSOLUTE:
                 err = float(torch.max(torch.abs(x - psi_m)).detach())
@@ -221,9 +338,10 @@ class Model:
         mi, mj = nx - 2, ny - 2
         n_int = mi * mj
         lid = torch.arange(n_int).reshape(mj, mi)
-        A = torch.zeros((n_int, n_int), dtype=T)
+        A = None if self.sparse else torch.zeros((n_int, n_int), dtype=T)
         cw, ce, cs, cn = cx * k["kw"], cx * k["ke"], cy * k["ks"], cy * k["kn"]
-        A = A + torch.diag((1.0 + cw + ce + cs + cn).reshape(-1))
+        if not self.sparse:
+            A = A + torch.diag((1.0 + cw + ce + cs + cn).reshape(-1))
         b = H[1:-1, 1:-1].clone()
         # neighbours: interior ones into A, ring ones into b
         for coef, dj, di in ((cw, 0, -1), (ce, 0, 1), (cs, -1, 0), (cn, 1, 0)):
@@ -232,11 +350,21 @@ class Model:
             inner = (nj >= 0) & (nj < mj) & (ni >= 0) & (ni < mi)
             rows = lid[jj[inner], ii[inner]]
             cols = lid[nj[inner], ni[inner]]
-            A = A.index_put((rows, cols), -coef[inner], accumulate=True)
+            if not self.sparse:
+                A = A.index_put((rows, cols), -coef[inner], accumulate=True)
             ringv = H[1:-1, 1:-1].new_zeros((mj, mi))
             Hr = H[1 + dj:ny - 1 + dj, 1 + di:nx - 1 + di]
             b = b + torch.where(~inner, coef * Hr, ringv)
-        x = torch.linalg.solve(A, b.reshape(-1)).reshape(mj, mi)
+        if self.sparse:
+            diag = 1.0 + cw + ce + cs + cn
+
+            def mv(v):
+                vp = F.pad(v, (1, 1, 1, 1))
+                return diag * v - cw * vp[1:-1, :-2] - ce * vp[1:-1, 2:] - cs * vp[:-2, 1:-1] - cn * vp[2:, 1:-1]
+            dd = diag.detach()
+            x = implicit_solve(mv, lambda r: r / dd, b, H[1:-1, 1:-1])
+        else:
+            x = torch.linalg.solve(A, b.reshape(-1)).reshape(mj, mi)
         Hn = H.clone()
         Hn = Hn.index_put((torch.arange(1, ny - 1)[:, None].expand(mj, mi), torch.arange(1, nx - 1)[None, :].expand(mj, mi)), x)
         # flow into the ring: implicit flux across the ring faces
@@ -255,13 +383,22 @@ class Model:
         thetan, Kn, _ = closure(psin, ks, al, nv, p.theta_s, p.theta_r)
         ph = self.h0
         thetas, qs, iters = [], [], []
-        for t in range(nsteps):
-            rain = self.rain[t] if t < len(self.rain) else 0.0
+        def step(psin, thetan, Kn, ph, ks, al, nv, rain):
             psin, thetan, Kn, ph, it = self.subsurface_step(psin, thetan, Kn, ph, rain, ks, al, nv)
             ph, q = self.overland_step(ph)
+            return psin, thetan, Kn, ph, q, torch.tensor(it)
+
+        for t in range(nsteps):
+            rain = self.rain[t] if t < len(self.rain) else 0.0
+            if self.checkpoint and torch.is_grad_enabled():
+                from torch.utils.checkpoint import checkpoint
+                psin, thetan, Kn, ph, q, it = checkpoint(step, psin, thetan, Kn, ph, ks, al, nv, rain,
+                                                         use_reentrant=False)
+            else:
+                psin, thetan, Kn, ph, q, it = step(psin, thetan, Kn, ph, ks, al, nv, rain)
             thetas.append(thetan)
             qs.append(q)
-            iters.append(it)
+            iters.append(int(it))
         return {"theta": thetas, "q": qs, "psi": psin, "ph": ph, "picard_iters": iters}
 
 
@@ -274,10 +411,10 @@ def loss_of(out, theta_target, q_target, w_q=1.0):
     return L
 
 
-def reference_gradient(domain, nsteps, theta_target, q_target, w_q=1.0):
+def reference_gradient(domain, nsteps, theta_target, q_target, w_q=1.0, sparse=False, checkpoint=False):
     """Loss and its gradient with respect to per-cell log Ks, alpha (1/m) and
     n, each in the reference 3D layout (k*nx*ny + j*nx + i)."""
-    m = Model(domain)
+    m = Model(domain, sparse=sparse, checkpoint=checkpoint)
     lk = m.logks0.clone().requires_grad_(True)
     al = m.alpha0.clone().requires_grad_(True)
     nv = m.n0.clone().requires_grad_(True)
@@ -287,9 +424,9 @@ def reference_gradient(domain, nsteps, theta_target, q_target, w_q=1.0):
     return float(L.detach()), lk.grad.reshape(-1).numpy(), al.grad.reshape(-1).numpy(), nv.grad.reshape(-1).numpy(), out
 
 
-def targets_from(domain, nsteps, logks=None, alpha=None, n=None):
+def targets_from(domain, nsteps, logks=None, alpha=None, n=None, sparse=False):
     """theta and Q_out series of a run (used to make a seeded target)."""
-    m = Model(domain)
+    m = Model(domain, sparse=sparse)
     with torch.no_grad():
         out = m.run(nsteps, logks, alpha, n)
     return [t.clone() for t in out["theta"]], [q.clone() for q in out["q"]]

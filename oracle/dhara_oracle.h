@@ -30,8 +30,10 @@ typedef struct dhara_oracle dhara_oracle;
 
 /* Linear solver used for the 3D system.  The reference runs unpreconditioned
  * CUSP BiCGSTAB (src/subsurface.cu:750-751); CG is offered for speed on the
- * symmetric all-Neumann matrix. */
-enum { ORACLE_SOLVER_BICGSTAB = 0, ORACLE_SOLVER_CG = 1 };
+ * symmetric all-Neumann matrix, and CG preconditioned by each column's
+ * vertical tridiagonal block for long horizons (same system, same stopping
+ * rule; the 2D overland system falls back to CG with it). */
+enum { ORACLE_SOLVER_BICGSTAB = 0, ORACLE_SOLVER_CG = 1, ORACLE_SOLVER_PCG_COLUMN = 2 };
 
 dhara_oracle *oracle_create(const dhara_params *p);
 void oracle_destroy(dhara_oracle *o);

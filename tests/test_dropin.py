@@ -1,8 +1,9 @@
 """The drop-in entry points (include/dhara_dropin.h) driven by a C++ host
 program written like the reference's host code (tests/dropin/dropin_driver.cc:
 reference struct layout, caller-allocated device arrays, one
-SubsurfaceFlowModel + OverlandFlowModel call per step), against the same
-steps through the Python path of the C ABI."""
+SubsurfaceFlowModel + OverlandFlowModel call per step), checked against the
+FP64 oracle of the reference algorithm on the same inputs, and against the
+same steps through the C ABI directly (the drop-in adds no arithmetic)."""
 import os
 import shutil
 import subprocess
@@ -13,6 +14,7 @@ import pytest
 
 import dhara_b200 as db
 from dhara_b200 import inputs
+import oracle
 
 from conftest import rel_err
 
@@ -30,7 +32,7 @@ def build_driver(tmp):
     return exe
 
 
-def test_dropin_matches_c_abi(gpu):
+def test_dropin_matches_oracle(gpu):
     nsteps = 4
     d = inputs.make_domain(20, 14, 8, seed=31, rain_mm_per_h=30.0, nsteps=nsteps, krylov_tol=1e-12,
                            krylov_maxiter=1000)
@@ -45,6 +47,14 @@ def test_dropin_matches_c_abi(gpu):
         out = subprocess.run([exe, tmp, str(nsteps)], capture_output=True, text=True, timeout=300)
         assert out.returncode == 0, out.stderr
         got = {k: np.fromfile(os.path.join(tmp, f"out_{k}.bin")) for k in ("psi", "theta", "ph", "H", "mb")}
+    # the reference algorithm (FP64 oracle, converged 3D solves)
+    o, od, _ = oracle.run(d, nsteps, solver3d=oracle.SOLVER_CG)
+    assert rel_err(got["psi"], o["psi"]) < 1e-7
+    assert rel_err(got["theta"], o["theta"]) < 1e-7
+    assert rel_err(got["H"], o["waterelev"]) < 1e-7
+    assert rel_err(got["ph"], o["ponding"]) < 1e-6
+    assert abs(got["mb"].sum() - od["mb_subsurface_cum"]) <= 1e-9 * max(1.0, abs(od["mb_subsurface_cum"]))
+    # and the drop-in is the C ABI's computation
     ref, dg, _ = db.run(d, nsteps=nsteps)
     assert rel_err(got["psi"], ref["psi"]) < 1e-12
     assert rel_err(got["theta"], ref["theta"]) < 1e-12

@@ -1,0 +1,90 @@
+"""GPU parity over the configured horizons, step by step ("shadowing").
+
+Before every step the FP64 oracle is given the state the GPU starts the step
+from; both advance one coupled step (SubsurfaceFlowModel + OverlandFlowModel,
+src/subsurface.cu:686-847 and src/overland.cu:387-419) and the end states are
+compared (oracle/shadow.py).  The largest one-step error over the whole
+trajectory is asserted, for the head psi, moisture theta, ponded depth and
+overland water elevation H:
+
+  32x32x20 workload, all 60 steps ........... FP64 1e-8, mixed 1e-4
+  64x64x40 patch of the 512x512x40 storm,
+    all 240 steps (mixed) / first 60 (FP64) . mixed 1e-4, FP64 1e-8
+
+Norm-wise relative errors max|gpu - oracle| / max|oracle|.  Free-running
+trajectories drift further apart than any one step (the scheme's discrete
+switches amplify rounding; tests/test_oracle_drift.py shows the oracle doing
+the same against itself), so the free-running GPU-vs-oracle difference is
+checked against the oracle's own spread instead.
+"""
+import numpy as np
+import pytest
+
+import dhara_b200 as db
+from dhara_b200 import inputs
+import oracle
+from oracle import shadow as sh
+
+pytestmark = pytest.mark.gpu
+
+
+def solver_for(d):
+    s = db.Solver(d.params)
+    s.load(d)
+    s.prepare()
+    return s
+
+
+def check(r, tol, tol_ponding=None):
+    m = r["max"]
+    print({k: f"{v:.3g}" for k, v in m.items()}, "picard mismatches:", r["picard_mismatch_steps"])
+    for k in ("psi", "theta", "waterelev"):
+        assert m[k] < tol, (k, m)
+    assert m["ponding"] < (tol if tol_ponding is None else tol_ponding), m
+
+
+@pytest.mark.parametrize("prec,tol", [(db.FP64, 1e-8), (db.MIXED, 1e-4)], ids=["fp64", "mixed"])
+def test_shadow_32x32x20_all_60_steps(gpu, prec, tol):
+    d = inputs.plain_fp64_32x32x20(precision=prec, krylov_tol=1e-12, krylov_maxiter=2000)
+    s = solver_for(d)
+    r = sh.shadow(s, d, 60)
+    s.close()
+    check(r, tol)
+    if prec == db.FP64:
+        assert r["picard_mismatch_steps"] == []
+
+
+def storm_patch(prec, nsteps):
+    return inputs.mixed_512x512x40(nx=64, ny=64, nz=40, precision=prec, nsteps=nsteps,
+                                   krylov_tol=1e-12, krylov_maxiter=2000)
+
+
+def test_shadow_storm_patch_all_240_steps_mixed(gpu):
+    d = storm_patch(db.MIXED, 240)
+    s = solver_for(d)
+    r = sh.shadow(s, d, 240)
+    s.close()
+    check(r, 1e-4)
+
+
+def test_shadow_storm_patch_fp64(gpu):
+    d = storm_patch(db.FP64, 60)
+    s = solver_for(d)
+    r = sh.shadow(s, d, 60)
+    s.close()
+    check(r, 1e-8)
+
+
+def test_free_run_drift_within_the_oracles_own_spread(gpu):
+    """60 free-running steps: the GPU ends as close to the oracle as the
+    oracle with a different (converged) overland solver ends to itself."""
+    d = inputs.plain_fp64_32x32x20(krylov_tol=1e-12, krylov_maxiter=2000)
+    g, _, _ = db.run(d, nsteps=60)
+    o, _, _ = oracle.run(d, 60, solver3d=oracle.SOLVER_PCG_COLUMN)
+    spread = sh.free_run_drift(d, 60, (oracle.SOLVER_PCG_COLUMN, oracle.SOLVER_BICGSTAB),
+                               (oracle.SOLVER_PCG_COLUMN, oracle.SOLVER_CG))
+    drift = {k: sh.rel_err(g[k], o[k]) for k in ("psi", "theta", "ponding", "waterelev")}
+    print("gpu drift", drift, "oracle spread", spread)
+    for k in drift:
+        assert drift[k] < 1e-3, (k, drift)
+        assert drift[k] <= 10 * max(spread[k], 1e-9), (k, drift, spread)
