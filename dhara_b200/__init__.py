@@ -82,6 +82,11 @@ def lib():
         "dhara_checkpoint": (ct.c_int, [vp, vp, ct.c_int64]),
         "dhara_restore": (ct.c_int, [vp, vp, ct.c_int64]),
         "dhara_selftest_bounded_wait": (ct.c_int, [ct.c_int, ct.c_double, P(ct.c_int)]),
+        "dhara_write_netcdf_state": (ct.c_int, [ct.c_char_p, ct.c_char_p, ct.c_int, ct.c_int, ct.c_int,
+                                                dp, dp, dp, dp]),
+        "dhara_write_netcdf_statistics": (ct.c_int, [ct.c_char_p, ct.c_char_p, ct.c_int, ct.c_int, dp, dp, dp]),
+        "dhara_save_netcdf_state": (ct.c_int, [vp, ct.c_int, ct.c_char_p, ct.c_char_p]),
+        "dhara_save_netcdf_statistics": (ct.c_int, [vp, ct.c_int, ct.c_char_p, ct.c_char_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -219,6 +224,20 @@ class Solver:
     def snapshot_wait(self):
         _check(lib().dhara_snapshot_wait(self.h))
 
+    def save_netcdf(self, file2d=None, file3d=None, domain=0):
+        """The reference's snapshot files (SaveModelResults, src/io.cc:854-906)
+        of the current state: water_elevation/water_depth and/or
+        pressure_head/moisture in NetCDF classic format."""
+        enc = lambda f: None if f is None else os.fsencode(f)
+        _check(lib().dhara_save_netcdf_state(self.h, domain, enc(file2d), enc(file3d)))
+
+    def save_netcdf_statistics(self, file1d=None, file_stat=None, domain=0):
+        """The reference's mb_subsurfaceW and pressure_mean/moisture_mean files
+        (SaveResultEntirePeriod, src/io.cc:962-996) from the statistics kept
+        since enable_statistics()."""
+        enc = lambda f: None if f is None else os.fsencode(f)
+        _check(lib().dhara_save_netcdf_statistics(self.h, domain, enc(file1d), enc(file_stat)))
+
     def apply_boundary_config(self, bc, domain=0):
         """Uploads the per-face settings of params_from_config's third result."""
         _check(lib().dhara_apply_boundary_config(self.h, domain, ct.byref(bc)))
@@ -330,6 +349,28 @@ def selftest_bounded_wait(limit_ms=200.0, device=0):
     out = ct.c_int(0)
     _check(lib().dhara_selftest_bounded_wait(device, float(limit_ms), ct.byref(out)))
     return bool(out.value)
+
+
+def write_netcdf_state(file2d, file3d, nx, ny, nz, water_elevation=None, water_depth=None,
+                       pressure_head=None, moisture=None):
+    """Writes host arrays (reference layout) as the reference's snapshot files;
+    host code only, no GPU needed."""
+    arrs = [None if a is None else np.ascontiguousarray(a, np.float64)
+            for a in (water_elevation, water_depth, pressure_head, moisture)]
+    enc = lambda f: None if f is None else os.fsencode(f)
+    _check(lib().dhara_write_netcdf_state(enc(file2d), enc(file3d), nx, ny, nz,
+                                          *[None if a is None else _dp(a) for a in arrs]))
+
+
+def write_netcdf_statistics(file1d, file_stat, nz, mb_subsurfaceW, pressure_sum, moisture_sum):
+    """Writes the reference's time-series and layer-statistics files from host
+    arrays ([nsteps] and [nsteps, nz]); host code only."""
+    mb = np.ascontiguousarray(mb_subsurfaceW, np.float64)
+    ps = np.ascontiguousarray(pressure_sum, np.float64)
+    th = np.ascontiguousarray(moisture_sum, np.float64)
+    enc = lambda f: None if f is None else os.fsencode(f)
+    _check(lib().dhara_write_netcdf_statistics(enc(file1d), enc(file_stat), mb.size, nz, _dp(mb), _dp(ps),
+                                               _dp(th)))
 
 
 def run(domains, nsteps=None, graph=False, record=(), device=0):

@@ -364,14 +364,13 @@ int build_tensor_maps(dhara_handle *h) {
         int rc = 0;
         rc |= encode_map(m + MAP_P0_H, P.p0, sT, D, true, chi);
         rc |= encode_map(m + MAP_P1_H, P.p1, sT, D, true, chi);
-        rc |= encode_map(m + MAP_Z_H, P.z, sT, D, true, chi);
+        rc |= encode_map(m + MAP_Z0_H, P.z0, sT, D, true, chi);
+        rc |= encode_map(m + MAP_Z1_H, P.z1, sT, D, true, chi);
+        rc |= encode_map(m + MAP_T0_H, P.t0, sT, D, true, chi);
+        rc |= encode_map(m + MAP_T1_H, P.t1, sT, D, true, chi);
         rc |= encode_map(m + MAP_K_H, P.K, sT, D, true, chi);
         rc |= encode_map(m + MAP_D_O, P.D, sT, D, false, chi);
         rc |= encode_map(m + MAP_DD_O, P.d, sT, D, false, chi);
-        rc |= encode_map(m + MAP_R_O, P.r, sT, D, false, chi);
-        rc |= encode_map(m + MAP_P0_O, P.p0, sT, D, false, chi);
-        rc |= encode_map(m + MAP_P1_O, P.p1, sT, D, false, chi);
-        rc |= encode_map(m + MAP_Q_O, P.q, sT, D, false, chi);
         rc |= encode_map(m + MAP_INV_O, P.finv, sT, D, false, chi);
         rc |= encode_map(m + MAP_C_O, P.fc, sT, D, false, chi);
         rc |= encode_map(m + MAP_X64_H, P.x, 8, D, true, CH_R);
@@ -585,6 +584,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         D.overland_tol = p.overland_tol;
         D.closure_fp32 = (h->mixed && p.closure_fp32) ? 1 : 0;
         D.closure_fast = (h->mixed && !p.closure_fp32) ? 1 : 0;
+        D.record_branches = p.record_branches ? 1 : 0;
         D.tile_begin = (int)h->htiles.size();
         for (int y0 = 0; y0 < p.ny; y0 += TILE_Y)
             for (int x0 = 0; x0 < p.nx; x0 += TILE_X) h->htiles.push_back({d, x0, y0, 0});
@@ -623,7 +623,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     TileDesc *d_tiles = nullptr;
     rc |= dalloc(h, &d_tiles, h->htiles.size());
     for (double **q : {&P.psin, &P.thetan, &P.psim, &P.x, &P.b, &P.ksat}) rc |= dalloc(h, q, N);
-    for (void **q : {&P.K, &P.D, &P.r, &P.p0, &P.p1, &P.z, &P.d, &P.q, &P.finv, &P.fc})
+    for (void **q : {&P.K, &P.D, &P.p0, &P.p1, &P.z0, &P.z1, &P.t0, &P.t1, &P.d, &P.finv, &P.fc})
         rc |= dalloc_void(h, q, N * sT);
     if (h->mixed) {
         rc |= dalloc(h, &P.K64, N);
@@ -686,7 +686,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     auto zero = [&](void *p, size_t bytes) { return cudaMemsetAsync(p, 0, bytes, h->stream); };
     cudaError_t e = cudaSuccess;
     for (double *q : {P.psin, P.thetan, P.psim, P.x, P.b, P.ksat}) e = e ? e : zero(q, N * 8);
-    for (void *q : {P.K, P.D, P.r, P.p0, P.p1, P.z, P.d, P.q, P.finv, P.fc}) e = e ? e : zero(q, N * sT);
+    for (void *q : {P.K, P.D, P.p0, P.p1, P.z0, P.z1, P.t0, P.t1, P.d, P.finv, P.fc}) e = e ? e : zero(q, N * sT);
     for (double *q : {P.K64, P.D64}) e = e ? e : zero(q, N * 8);
     for (double *q : {P.ztopo, P.mann, P.h, P.H, P.ph, P.ppt, P.esoil, P.tr, P.hpoten, P.qtop, P.ktop, P.bcqb,
                       P.olf_b, P.olf_r, P.olf_p0, P.olf_p1, P.olf_z, P.olf_w, P.olf_s, P.olf_p})
@@ -1100,6 +1100,7 @@ int dhara_get_diagnostics(dhara_handle *h, int domain, dhara_diagnostics *out) {
     out->ponded_volume = dg.ponded;
     out->picard_err_last = pc.err;
     out->krylov_relres_last = dg.krylov_relres_last;
+    out->branch_signature = dg.branch_sig;
     return rc;
 }
 
@@ -1162,13 +1163,14 @@ int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations
         const double solves = (double)dg.picard_iters_total;
         const double cycles = (double)dg.refine_iters_total;
         const double upd = cycles > solves ? cycles - solves : 0.0;
-        // inner iteration: phase A reads z, p_old, K, D and writes p, q (6 T-words);
-        // phase B reads p, q, d, r, 1/den, c' and writes d, r, z (9; the back
-        // sweep's second read of c' follows the staged read and is not counted);
-        // outer residual R: x, b, K64, D64 (f64) + writes r, z and the two
-        // factors (4 T) + c' read back (1 T); update U: x read+write (f64) + d (T).
-        total += N * (15.0 * sT * (double)dg.krylov_iters_total + (32.0 + 5.0 * sT) * cycles +
-                      (16.0 + sT) * upd);
+        // inner iteration (one sweep): reads the previous z, t, p and K, D,
+        // 1/den, c', d and writes z, t, p, d (12 T-words; the back sweep's second
+        // read of c' follows the staged read and is not counted); the first
+        // sweep of a cycle reads no previous t, p or d (3 words fewer).  Outer
+        // residual R: x, b, K64, D64 (f64) + writes z and the two factors (3 T)
+        // + c' read back (1 T); update U: x read+write (f64) + d, p (2 T).
+        total += N * (12.0 * sT * (double)dg.krylov_iters_total - 3.0 * sT * upd +
+                      (32.0 + 4.0 * sT) * cycles + (16.0 + 2.0 * sT) * upd);
         iters += dg.krylov_iters_total;
     }
     if (bytes) *bytes = total;

@@ -212,6 +212,49 @@ __device__ __forceinline__ bool domain_reduce(const DevPtrs &P, int tile, int do
     return true;
 }
 
+// ---------------------------------------------------- branch signature
+// An order-independent record of discrete decisions: each decision of kind
+// `kind` at `step`, entity `index` with outcome `code` contributes
+// mix(step, kind, index, code) to a 64-bit sum (mod 2^64), so two runs that
+// took the same decisions everywhere have equal sums and any differing
+// decision changes the sum (barring a 2^-64 coincidence).  mix is the
+// splitmix64 finaliser (Steele, Lea & Flood 2014).
+enum { BR_TOPFLUX = 1, BR_PONDCLIP = 2, BR_MANNING = 3, BR_DEPTHCLIP = 4, BR_SATURATION = 5, BR_PICARD = 6 };
+
+__device__ __forceinline__ unsigned long long branch_mix(int step, int kind, long long index, unsigned code) {
+    unsigned long long x = ((unsigned long long)(unsigned)step << 40) ^ ((unsigned long long)kind << 36) ^
+                           (unsigned long long)index ^ ((unsigned long long)code * 0x9e3779b97f4a7c15ull);
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+// Outcome of the comparison a > b as 0 (below), 1 (within `band` of the
+// boundary) or 2 (above).  Decisions are recorded in these three states so
+// that a comparison that sits on its boundary up to rounding (a ponding
+// clip of exactly the infiltrated depth, a dry cell's H - z) records the same
+// state in two runs whatever its rounding; only a move across a band edge
+// changes the record.
+__device__ __forceinline__ unsigned band3(double a, double b, double band) {
+    const double d = a - b;
+    return d > band ? 2u : (d < -band ? 0u : 1u);
+}
+// band for comparing two values of magnitude ~|a|, |b|: relative 1e-9, plus an absolute floor
+__device__ __forceinline__ double rel_band(double a, double b, double floor_abs) {
+    return 1e-9 * (fabs(a) + fabs(b)) + floor_abs;
+}
+
+// Adds every thread's v to *sig: warp sums, one atomic per warp.  All threads
+// of the warp must call it (v = 0 where a thread has nothing to add).
+__device__ __forceinline__ void branch_commit(unsigned long long *sig, unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(sig, v);
+}
+
 // ------------------------------------------------------- math wrappers
 template <typename T> __device__ __forceinline__ T m_log(T x);
 template <> __device__ __forceinline__ double m_log(double x) { return log(x); }

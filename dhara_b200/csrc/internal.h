@@ -18,20 +18,43 @@
 #define TILE_Y 4
 #define TILE_THREADS (TILE_X * TILE_Y)
 #define NZ_MAX 64
-// planes per TMA-staged chunk: inner phases (by inner precision) and the FP64 residual
-#define CHUNK_F32 3
-#define CHUNK_F64 4
+// planes per TMA-staged chunk: inner sweep (by inner precision) and the FP64
+// residual (compile-time; -D overrides them for timing alternatives)
+#ifndef CHUNK_F32
+#define CHUNK_F32 2
+#endif
+#ifndef CHUNK_F64
+#define CHUNK_F64 2
+#endif
+#ifndef CH_R
 #define CH_R 2
+#endif
 // TMA staging buffers per block (chunks in flight ahead of the one being computed: STAGES - 1)
+#ifndef STAGES
 #define STAGES 2
+#endif
+// Krylov kernel: blocks per SM it is compiled for (register budget), and
+// whether the FP32 column solve keeps its forward-sweep values d' in shared
+// memory (1) or in the t array it then overwrites (0)
+#ifndef KRYLOV_BLOCKS_F32
+#define KRYLOV_BLOCKS_F32 5
+#endif
+#ifndef KRYLOV_BLOCKS_F64
+#define KRYLOV_BLOCKS_F64 4
+#endif
+#ifndef KRYLOV_DSMEM_F32
+#define KRYLOV_DSMEM_F32 1
+#endif
 
 // Tensor maps of one domain (index = dom * NMAP + id): halo boxes
 // (TILE_X + 32 bytes) x (TILE_Y + 2) x chunk, own boxes TILE_X x TILE_Y x chunk.
+// The inner iteration's vectors z, t = M^-1 A p and p are double buffered
+// (the sweep reads the previous iteration's at the halo and writes the new
+// one's at its own columns).
 enum {
-    MAP_P0_H = 0, MAP_P1_H, MAP_Z_H, MAP_K_H,      // inner precision, halo boxes
-    MAP_D_O, MAP_DD_O, MAP_R_O,                    // inner precision, own boxes (D, d, r)
-    MAP_P0_O, MAP_P1_O, MAP_Q_O, MAP_INV_O, MAP_C_O,  // inner precision, own boxes
-    MAP_X64_H, MAP_K64_H, MAP_D64_O, MAP_B_O,      // FP64 outer residual
+    MAP_P0_H = 0, MAP_P1_H, MAP_Z0_H, MAP_Z1_H, MAP_T0_H, MAP_T1_H, MAP_K_H,  // inner precision, halo
+    MAP_D_O, MAP_DD_O, MAP_INV_O, MAP_C_O,                                    // inner precision, own
+    MAP_X64_H, MAP_K64_H, MAP_D64_O, MAP_B_O,                                 // FP64 outer residual
     NMAP
 };
 
@@ -46,6 +69,7 @@ struct DomainDesc {
     int krylov_maxiter, inner_maxiter, overland_maxiter, sched_len;
     int tile_begin, tile_end, closure_fp32, nxp;  // nxp: row pitch of 3D arrays (nx rounded up to 4)
     int closure_fast, has_dirichlet;              // reformulated FP64 closure (mixed mode); any type-0 face
+    int record_branches, pad_rb;                  // accumulate DevDiag::branch_sig
     long long off3, off2, offWE, offSN, sched_off;
     double dx, dy, dz, dt;
     double alpha, n, theta_s, theta_r, porosity, Ss, am;
@@ -63,16 +87,15 @@ struct TileDesc {
 struct KrylovCtrl {
     double bb;          // ||b||^2 of the 3D system
     double rr64;        // ||b - A x||^2 at the last outer check
-    double rr;          // inner residual^2
-    double rz;          // preconditioned inner product r.z
-    double alpha, beta;
-    double inner_target2;
+    double rz;          // preconditioned residual norm r.M^-1 r after the last inner iteration
+    double alpha, beta; // step of the last inner iteration (its x update is pending) and the next beta
+    double inner_target2;  // the inner solve stops when rz falls to this
     int active;         // outer solve still running
     int inner_active;   // inner PCG running
     int inner_iter;     // inner iterations in the current cycle
     int total_iter;     // inner iterations this solve
     int cycles;         // outer residual recomputes this solve
-    int parity;         // which p buffer holds the current direction
+    int parity;         // which z/t/p buffers hold the last iteration's vectors
     int first_inner;
     int pad;
 };
@@ -123,6 +146,7 @@ struct DevDiag {
     int overland_nonconverged, nonfinite, pad0, pad1;
     double mb_last, mb_cum, storage_cum, top_cum, bottom_cum, rain_cum;
     double olf_out_cum, olf_clip_cum, ponded, picard_err_last, krylov_relres_last;
+    unsigned long long branch_sig;  // hash-sum of the run's discrete decisions (record_branches)
 };
 
 struct GridBarrier {
@@ -156,11 +180,11 @@ struct DevPtrs {
     double *psin, *thetan, *psim, *x, *b, *ksat, *alpha, *nvg;
     // FP64 coefficients of the outer residual (alias K, D in FP64 mode)
     double *K64, *D64;
-    // 3D inner-precision buffers
-    void *K, *D, *r, *p0, *p1, *z, *d;
-    // A p of the current direction, and the column preconditioner's stored
+    // 3D inner-precision buffers: stencil coefficients, the inner solve's
+    // double-buffered z (preconditioned residual), t = M^-1 A p and p, its
+    // solution increment d, and the column preconditioner's stored
     // L D L^T factors (1/den, c' = c/den), computed once per outer cycle
-    void *q, *finv, *fc;
+    void *K, *D, *p0, *p1, *z0, *z1, *t0, *t1, *d, *finv, *fc;
     // 2D double
     double *ztopo, *mann, *h, *H, *ph, *ppt, *esoil, *tr, *hpoten, *qtop, *ktop, *bcqb;
     double *olf_k;       // 4*C: kw, ke, ks, kn per column (row-based)

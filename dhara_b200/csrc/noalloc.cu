@@ -2,9 +2,8 @@
 //
 // Some callers cannot allocate device memory when they need a step: a host
 // application that hands the library only the arrays it owns (a plugin inside
-// a model that manages all GPU memory itself), code running while a CUDA
-// stream is being captured into a graph (cudaMalloc is not allowed during
-// capture), or a real-time loop that forbids allocation after start-up.  For
+// a model that manages all GPU memory itself and has no spare memory to give),
+// or a real-time loop that forbids allocation after start-up.  For
 // them dhara_overland_step_noalloc performs one overland step -- the same
 // computation as dhara_overland_step for one domain -- on the caller's device
 // arrays, and keeps all of its scratch (the four Manning conductances and the
@@ -19,8 +18,14 @@
 //    different host threads, without ordering between them) race on it and
 //    produce wrong results: order them on one stream.
 //  * The first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (once per device, that device current).  Make that
-//    first call before any stream capture begins.
+//    cudaGetSymbolAddress (once per device, that device current) and caches
+//    it for the life of the process.  Make that first call before any stream
+//    capture begins, and do not call the entry point again on a device after
+//    cudaDeviceReset (the cached address then belongs to the old context).
+//  * The four arrays must not overlap, except ztopo with mann (both read).
+//  * Convergence is not reported: the solve stops at overland_tol or after
+//    overland_maxiter iterations, whichever comes first, and returns
+//    DHARA_OK either way (the handle-based path counts unconverged solves).
 //  * The solve runs in a single thread block, so it suits small domains; the
 //    handle-based path is the fast one for large grids.
 #include <cstdio>
@@ -212,6 +217,20 @@ extern "C" int dhara_overland_step_noalloc(const dhara_params *p, double *waterd
                  "dhara_overland_step_noalloc: %d x %d = %lld columns exceeds the fixed scratch of %d columns",
                  p->nx, p->ny, (long long)p->nx * p->ny, DHARA_NOALLOC_MAX_COLUMNS);
         return na_fail(DHARA_ERR_UNSUPPORTED, buf);
+    }
+    // The two written arrays must not overlap each other or the inputs: the
+    // set-up writes H while neighbouring threads still read h, z and n.
+    {
+        const size_t bytes = (size_t)p->nx * p->ny * sizeof(double);
+        auto overlap = [bytes](const void *x, const void *y) {
+            const char *a0 = (const char *)x, *b0 = (const char *)y;
+            return a0 < b0 + bytes && b0 < a0 + bytes;
+        };
+        if (overlap(waterelev, waterdepth) || overlap(waterelev, ztopo) || overlap(waterelev, mann) ||
+            overlap(waterdepth, ztopo) || overlap(waterdepth, mann))
+            return na_fail(DHARA_ERR_INVALID,
+                           "dhara_overland_step_noalloc: waterdepth and waterelev must not overlap each other, "
+                           "ztopo or mann");
     }
     void *scratch = nullptr;
     const int rc = scratch_address(&scratch);

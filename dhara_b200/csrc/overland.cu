@@ -20,9 +20,13 @@ __device__ __forceinline__ bool is_ring(int i, int j, int nx, int ny) {
 
 // Manning conductance of one face (src/overland.cu:279-297 and the three
 // analogous blocks): the depth test is upwinded on the water elevation.
+// `code` receives the test's three comparisons in three states each (band3;
+// depths and slopes are compared to 1e-9 m and 1e-9, the overland solve's
+// rounding level), for the branch signature.
 __device__ __forceinline__ double manning_k(double Hnb, double hnb, double mnb, double Hc, double hc,
-                                            double mc, double S, const DomainDesc &D) {
+                                            double mc, double S, const DomainDesc &D, unsigned &code) {
     const double hup = (Hnb > Hc) ? hnb : hc;
+    code = (band3(hup, D.hmin, 1e-9) * 3u + band3((hnb + hc) / 2., D.hmin, 1e-9)) * 3u + band3(fabs(S), D.delta, 1e-9);
     if (hup > D.hmin && (hnb + hc) / 2. > D.hmin && fabs(S) > D.delta)
         return pow((hnb + hc) / 2., 5. / 3.) / (0.5 * (mnb + mc) * sqrt(S));
     return D.K0;
@@ -45,40 +49,46 @@ __global__ void __launch_bounds__(TILE_THREADS) k_olf_setup(DevPtrs P, long long
         P.gctrl->olf_bar = 0;
     }
     const ColumnRef cr = column_of(P, tile);
-    if (!cr.valid) return;
-    const int N = cr.nx, M = cr.ny, i = cr.i, j = cr.j;
-    const long long I = cr.c;
-    const double *h = P.h, *z = P.ztopo, *mann = P.mann;
-    auto Hs = [&](long long q) { return h[q] + z[q]; };
-    const double h_ = h[I], Hs_ = Hs(I), mann_ = mann[I];
-    P.H[I] = Hs_;
-    P.olf_b[I] = Hs_;
-    double kw = 0, ke = 0, ks = 0, kn = 0;
-    if (!is_ring(i, j, N, M)) {
-        const double h_p1 = h[I + 1], Hs_p1 = Hs(I + 1), mann_p1 = mann[I + 1];
-        const double h_m1 = h[I - 1], Hs_m1 = Hs(I - 1), mann_m1 = mann[I - 1];
-        const double h_pN = h[I + N], Hs_pN = Hs(I + N), mann_pN = mann[I + N];
-        const double h_mN = h[I - N], Hs_mN = Hs(I - N), mann_mN = mann[I - N];
-        const double Hs_pNp1 = Hs(I + N + 1), Hs_pNm1 = Hs(I + N - 1);
-        const double Hs_mNp1 = Hs(I - N + 1), Hs_mNm1 = Hs(I - N - 1);
-        const double dx = D.dx, dy = D.dy;
-        const double Sse = sqrt(pow((Hs_p1 - Hs_) / dx, 2.) +
-                                pow((Hs_pNp1 + Hs_pN - Hs_mNp1 - Hs_mN) / (4 * dy), 2.));
-        ke = manning_k(Hs_p1, h_p1, mann_p1, Hs_, h_, mann_, Sse, D);
-        const double Ssw = sqrt(pow((Hs_ - Hs_m1) / dx, 2.) +
-                                pow((Hs_pN + Hs_pNm1 - Hs_mN - Hs_mNm1) / (4 * dy), 2.));
-        kw = manning_k(Hs_m1, h_m1, mann_m1, Hs_, h_, mann_, Ssw, D);
-        const double Ssn = sqrt(pow((Hs_pN - Hs_) / dy, 2.) +
-                                pow((Hs_pNp1 + Hs_p1 - Hs_pNm1 - Hs_m1) / (4 * dx), 2.));
-        kn = manning_k(Hs_pN, h_pN, mann_pN, Hs_, h_, mann_, Ssn, D);
-        const double Sss = sqrt(pow((Hs_ - Hs_mN) / dy, 2.) +
-                                pow((Hs_p1 + Hs_mNp1 - Hs_m1 - Hs_mNm1) / (4 * dx), 2.));
-        ks = manning_k(Hs_mN, h_mN, mann_mN, Hs_, h_, mann_, Sss, D);
+    unsigned long long bsig = 0;
+    if (cr.valid) {
+        const int N = cr.nx, M = cr.ny, i = cr.i, j = cr.j;
+        const long long I = cr.c;
+        const double *h = P.h, *z = P.ztopo, *mann = P.mann;
+        auto Hs = [&](long long q) { return h[q] + z[q]; };
+        const double h_ = h[I], Hs_ = Hs(I), mann_ = mann[I];
+        P.H[I] = Hs_;
+        P.olf_b[I] = Hs_;
+        double kw = 0, ke = 0, ks = 0, kn = 0;
+        if (!is_ring(i, j, N, M)) {
+            const double h_p1 = h[I + 1], Hs_p1 = Hs(I + 1), mann_p1 = mann[I + 1];
+            const double h_m1 = h[I - 1], Hs_m1 = Hs(I - 1), mann_m1 = mann[I - 1];
+            const double h_pN = h[I + N], Hs_pN = Hs(I + N), mann_pN = mann[I + N];
+            const double h_mN = h[I - N], Hs_mN = Hs(I - N), mann_mN = mann[I - N];
+            const double Hs_pNp1 = Hs(I + N + 1), Hs_pNm1 = Hs(I + N - 1);
+            const double Hs_mNp1 = Hs(I - N + 1), Hs_mNm1 = Hs(I - N - 1);
+            const double dx = D.dx, dy = D.dy;
+            unsigned we, ww, wn, ws;
+            const double Sse = sqrt(pow((Hs_p1 - Hs_) / dx, 2.) +
+                                    pow((Hs_pNp1 + Hs_pN - Hs_mNp1 - Hs_mN) / (4 * dy), 2.));
+            ke = manning_k(Hs_p1, h_p1, mann_p1, Hs_, h_, mann_, Sse, D, we);
+            const double Ssw = sqrt(pow((Hs_ - Hs_m1) / dx, 2.) +
+                                    pow((Hs_pN + Hs_pNm1 - Hs_mN - Hs_mNm1) / (4 * dy), 2.));
+            kw = manning_k(Hs_m1, h_m1, mann_m1, Hs_, h_, mann_, Ssw, D, ww);
+            const double Ssn = sqrt(pow((Hs_pN - Hs_) / dy, 2.) +
+                                    pow((Hs_pNp1 + Hs_p1 - Hs_pNm1 - Hs_m1) / (4 * dx), 2.));
+            kn = manning_k(Hs_pN, h_pN, mann_pN, Hs_, h_, mann_, Ssn, D, wn);
+            const double Sss = sqrt(pow((Hs_ - Hs_mN) / dy, 2.) +
+                                    pow((Hs_p1 + Hs_mNp1 - Hs_m1 - Hs_mNm1) / (4 * dx), 2.));
+            ks = manning_k(Hs_mN, h_mN, mann_mN, Hs_, h_, mann_, Sss, D, ws);
+            if (D.record_branches)
+                bsig = branch_mix(P.pctrl[td.dom].step, BR_MANNING, I, ((we * 27u + ww) * 27u + wn) * 27u + ws);
+        }
+        P.olf_k[0 * ctot + I] = kw;
+        P.olf_k[1 * ctot + I] = ke;
+        P.olf_k[2 * ctot + I] = ks;
+        P.olf_k[3 * ctot + I] = kn;
     }
-    P.olf_k[0 * ctot + I] = kw;
-    P.olf_k[1 * ctot + I] = ke;
-    P.olf_k[2 * ctot + I] = ks;
-    P.olf_k[3 * ctot + I] = kn;
+    if (D.record_branches) branch_commit(&P.diag[td.dom].branch_sig, bsig);
 }
 
 struct OlfRow {
@@ -651,6 +661,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_olf_finish(DevPtrs P, long lon
     if (tile == 0 && threadIdx.x == 0) P.gctrl->n_olf_active = 0;
     const ColumnRef cr = column_of(P, tile);
     double v[3] = {0, 0, 0};  // boundary out, clip, ponded
+    unsigned long long bsig = 0;
     if (cr.valid) {
         const long long I = cr.c;
         const double H = P.H[I];
@@ -659,6 +670,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_olf_finish(DevPtrs P, long lon
         P.h[I] = hn;
         P.ph[I] = hn;
         if (d < 0) v[1] = -d;
+        if (D.record_branches) bsig = branch_mix(P.pctrl[td.dom].step, BR_DEPTHCLIP, I, band3(d, 0.0, 1e-9));
         v[2] = hn;
         if (!is_ring(cr.i, cr.j, cr.nx, cr.ny)) {
             const OlfRow w = olf_row(P, cr, D, ctot);
@@ -668,6 +680,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_olf_finish(DevPtrs P, long lon
             if (cr.j == cr.ny - 2) v[0] += w.cy * w.kn * (H - P.H[I + cr.nx]);
         }
     }
+    if (D.record_branches) branch_commit(&P.diag[td.dom].branch_sig, bsig);
     if (domain_reduce<3>(P, tile, td.dom, 3, v) && threadIdx.x == 0) {
         DevDiag &dg = P.diag[td.dom];
         const OverlandCtrl &oc = P.octrl[td.dom];

@@ -65,6 +65,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
 // Waits for the chunk of buffer b; gives up after MBAR_TIMEOUT_NS and raises
 // the handle's error flag (the grid barrier then ends the kernel).
 #define MBAR_TIMEOUT_NS 2000000000ull
+#define DRAIN_TIMEOUT_NS 500000000ull
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, GridBarrier *gb) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*(volatile int *)&gb->error) return false;
@@ -114,15 +115,35 @@ constexpr unsigned halo_slot() {
     return (halo_bytes<V, CHN>() + 127u) & ~127u;
 }
 
-// Block-uniform state of the two staging buffers: mbarriers and the parity
-// each buffer's next completion will have.
+// Block-uniform state of the staging buffers: mbarriers and the parity each
+// buffer's next completion will have.  `pending` (meaningful in thread 0, the
+// one that issues) marks buffers with a copy issued and not yet consumed.
 struct StageBars {
-    uint64_t *bar;      // bar[0], bar[1] in shared memory
+    uint64_t *bar;      // bar[0 .. STAGES-1] in shared memory
     unsigned parity;    // bit b: expected parity of buffer b
     GridBarrier *gb;
+    unsigned pending;
+    __device__ __forceinline__ void issued(int b) { pending |= 1u << b; }
+    // A wait that gives up leaves its buffer pending, with the parity it was
+    // waiting for, so drain() can still wait for that copy.
     __device__ __forceinline__ bool wait(int b) {
         const bool ok = mbar_wait(bar + b, (parity >> b) & 1u, gb);
-        parity ^= 1u << b;
+        if (ok) {
+            parity ^= 1u << b;
+            pending &= ~(1u << b);
+        }
         return ok;
+    }
+    // On an error exit: waits, bounded by DRAIN_TIMEOUT_NS per buffer, for
+    // every copy this thread issued and nothing consumed, so no TMA write
+    // into the block's shared memory is in flight when the block exits.
+    __device__ __forceinline__ void drain() {
+        for (int b = 0; b < STAGES; ++b) {
+            if (!((pending >> b) & 1u)) continue;
+            const unsigned long long t0 = global_ns();
+            while (!mbar_try_wait(bar + b, (parity >> b) & 1u) && global_ns() - t0 < DRAIN_TIMEOUT_NS) {
+            }
+        }
+        pending = 0;
     }
 };

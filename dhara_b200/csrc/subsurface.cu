@@ -108,31 +108,42 @@ __global__ void k_prologue(DevPtrs P) {
             for (int q = 0; q < 16; ++q) P.step_acc[td.dom * 16 + q] = 0.0;
         }
     }
-    if (!cr.valid) return;
-    const long long c = cr.c, g = cr.g0;  // top cell k = 0
-    const double dt = D.dt, dz = D.dz;
-    const int step = P.pctrl[td.dom].step;
-    double ppt;
-    if (D.sched_len > 0)
-        ppt = (step < D.sched_len) ? P.rain_sched[D.sched_off + step] : 0.0;
-    else
-        ppt = P.ppt[c];
-    P.ppt[c] = ppt;
-    const double ph = P.ph[c];
-    const double hpoten = ph + ppt / 1000 - P.esoil[c] * D.sec * dt;
-    const double ks = P.ksat[g];
-    double qcapa = -P.ktop[c] * ((P.psin[g] - hpoten - 0.5 * dz) / (0.5 * dz));
-    if (ph / dt > ks) qcapa = fmax(qcapa, ks);
-    double q;
-    if (hpoten > 0.0) {
-        q = (hpoten / dt > qcapa) ? qcapa : hpoten / dt;
-        q = fmin(q, (D.theta_s - P.thetan[g]) * dz / dt);
-        q = fmin(q, ks);
-    } else {
-        q = hpoten / dt;
+    unsigned long long bsig = 0;
+    if (cr.valid) {
+        const long long c = cr.c, g = cr.g0;  // top cell k = 0
+        const double dt = D.dt, dz = D.dz;
+        const int step = P.pctrl[td.dom].step;
+        double ppt;
+        if (D.sched_len > 0)
+            ppt = (step < D.sched_len) ? P.rain_sched[D.sched_off + step] : 0.0;
+        else
+            ppt = P.ppt[c];
+        P.ppt[c] = ppt;
+        const double ph = P.ph[c];
+        const double hpoten = ph + ppt / 1000 - P.esoil[c] * D.sec * dt;
+        const double ks = P.ksat[g];
+        double qcapa = -P.ktop[c] * ((P.psin[g] - hpoten - 0.5 * dz) / (0.5 * dz));
+        // which branches the selection took, each comparison in three states (band3)
+        unsigned code = band3(ph / dt, ks, rel_band(ph / dt, ks, 1e-30));
+        if (ph / dt > ks) qcapa = fmax(qcapa, ks);
+        double q;
+        code = code * 3u + band3(hpoten, 0.0, 1e-15);
+        if (hpoten > 0.0) {
+            code = code * 3u + band3(hpoten / dt, qcapa, rel_band(hpoten / dt, qcapa, 1e-30));
+            q = (hpoten / dt > qcapa) ? qcapa : hpoten / dt;
+            const double room = (D.theta_s - P.thetan[g]) * dz / dt;
+            code = code * 3u + band3(q, room, rel_band(q, room, 1e-30));
+            q = fmin(q, room);
+            code = code * 3u + band3(q, ks, rel_band(q, ks, 1e-30));
+            q = fmin(q, ks);
+        } else {
+            q = hpoten / dt;
+        }
+        P.hpoten[c] = hpoten;
+        P.qtop[c] = q;
+        if (D.record_branches) bsig = branch_mix(step, BR_TOPFLUX, c, code);
     }
-    P.hpoten[c] = hpoten;
-    P.qtop[c] = q;
+    if (D.record_branches) branch_commit(&P.diag[td.dom].branch_sig, bsig);
 }
 
 // -------------------------------------------------------------- assembly
@@ -167,6 +178,18 @@ __global__ void __launch_bounds__(TILE_THREADS, 8) k_assemble(DevPtrs P) {
     }
     if (done) return;
     const ColumnRef cr = column_of(P, tile);
+    if (D.record_branches) {
+        // saturation (psi >= 0 switches the closure's branch) of every cell at psi^m
+        unsigned long long bsig = 0;
+        if (cr.valid) {
+            long long g = cr.g0;
+            for (int k = 0; k < cr.nz; ++k, g += cr.sxy) {
+                const double psi = (iter == 0) ? P.psin[g] : D.am * P.psim[g] + (1.0 - D.am) * P.x[g];
+                bsig += branch_mix(pc.step * 64 + (iter & 63), BR_SATURATION, g, band3(psi, 0.0, 1e-9));
+            }
+        }
+        branch_commit(&P.diag[td.dom].branch_sig, bsig);
+    }
     if (!cr.valid) return;
     const int nz = cr.nz;
     const double dt = D.dt, dz = D.dz, dx = D.dx, dy = D.dy;
@@ -374,18 +397,35 @@ __global__ void __launch_bounds__(TILE_THREADS) k_dir_rows(DevPtrs P) {
 // Persistent cooperative kernel: for every active domain it solves
 // A x = b to ||b - A x|| <= tol ||b|| (the CUSP monitor's rule,
 // CUSP/detail/monitor.inl:108-111,181-201) by iterative refinement:
-//   R: r = b - A x in FP64 arithmetic, r_T = (T) r, z = M^-1 r_T
-//   inner PCG in T on A d = r_T, M = the z-line (column) tridiagonal part of A
+//   R: r = b - A x in FP64 arithmetic, z = M^-1 (T) r
+//   inner PCG in T on A d = (T) r, M = the z-line (column) tridiagonal part of A
 //   U: x += d
 // In FP64 mode T = double and one cycle normally converges (the inner target
 // is the outer tolerance).  In mixed mode T = float, the inner solve reduces
 // the residual by inner_tol and cycles repeat until the FP64 residual meets
 // the tolerance.  The reference runs unpreconditioned BiCGSTAB; any solver
 // converged to the same tolerance yields the same head field.
-struct KrylovPhaseArgs {
-    int nz, i, j, nx, ny;
-    long long g0, sxy;
-};
+//
+// One inner PCG iteration is ONE sweep and one grid barrier.  The residual r
+// and A p are never stored: the sweep carries the preconditioned residual z
+// and t = M^-1 A p, whose recurrence z_{i+1} = z_i - alpha_i t_i is the
+// residual's r_{i+1} = r_i - alpha_i A p_i mapped through M^-1.  Sweep i
+// (alpha_{i-1}, beta_i known from the previous reduction):
+//   z_i = z_{i-1} - alpha_{i-1} t_{i-1},  p_i = z_i + beta_i p_{i-1}
+//       (formed at the tile's own and halo columns from the staged previous
+//       z, t, p, so no neighbour has to publish them first)
+//   q = A p_i,  t_i = M^-1 q (column solve),  d += alpha_{i-1} p_{i-1}
+//   partial sums sigma = p_i.q, mu = z_i.q, nu = q.t_i, rho_i = z_i.M z_i
+// and after the barrier alpha_i = rho_i / sigma and
+//   rho_{i+1} = rho_i - 2 alpha_i mu + alpha_i^2 nu    (r_i.t_i = z_i.q by
+//   symmetry of M), beta_{i+1} = rho_{i+1} / rho_i.
+// rho_i is evaluated directly from z_i (M z is column-local) rather than
+// carried by the update formula, which would accumulate cancellation; the
+// formula is only ever applied to a freshly computed rho.  x's last update
+// (alpha of the final iteration times its p) is applied in U.
+// Per inner iteration each cell reads z, t, p, K (at the halo), D, 1/den, c',
+// d and writes z, t, p, d: 12 words, against 15 and two grid barriers for the
+// textbook two-phase iteration.
 
 template <typename T>
 struct StencilW {
@@ -403,13 +443,11 @@ struct Chunk {
 template <typename T>
 struct StageSize {
     static constexpr int C = Chunk<T>::inner;
-    // phase A: z, p_old, K (halo); D (own)
-    static constexpr size_t A = 3 * (size_t)halo_slot<T, C>() + own_bytes<T, C>();
-    // phase B: p, q, d, r, 1/den, c' (own)
-    static constexpr size_t B = 6 * (size_t)own_bytes<T, C>();
+    // inner sweep: z, t, p of the previous iteration and K (halo); D, 1/den, c', d (own)
+    static constexpr size_t I = 4 * (size_t)halo_slot<T, C>() + 4 * (size_t)own_bytes<T, C>();
     // phase R: x, K64 (halo); D64, b (own), all FP64
     static constexpr size_t R = 2 * (size_t)halo_slot<double, CH_R>() + 2 * (size_t)own_bytes<double, CH_R>();
-    static constexpr size_t buffer() { return A > B ? (A > R ? A : R) : (B > R ? B : R); }
+    static constexpr size_t buffer() { return I > R ? I : R; }
     static constexpr size_t bytes() { return STAGES * buffer(); }
 };
 
@@ -528,6 +566,7 @@ __device__ __forceinline__ void issue_R(const DevPtrs &P, int tile, int st, int 
     const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
     unsigned char *B = stage + b * StageSize<T>::buffer();
     const int k0 = st * CHN;
+    sb.issued(b);
     mbar_expect_tx(sb.bar + b, 2 * HB + 2 * OB);
     tma_halo<double, CHN>((double *)B, maps + MAP_X64_H, td.x0, td.y0, k0, sb.bar + b);
     tma_halo<double, CHN>((double *)(B + HS), maps + MAP_K64_H, td.x0, td.y0, k0, sb.bar + b);
@@ -535,9 +574,12 @@ __device__ __forceinline__ void issue_R(const DevPtrs &P, int tile, int st, int 
     tma_own<double, CHN>((double *)(B + 2 * HS + OB), maps + MAP_B_O, td.x0, td.y0, k0, sb.bar + b);
 }
 
+// The inner sweep's chunk: the previous iteration's z, t, p (buffers `prev`)
+// and K at the halo, D, 1/den, c' and d at the own columns.  The first sweep of
+// a cycle has no previous t, p or d (alpha = beta = 0, d starts at zero).
 template <typename T>
-__device__ __forceinline__ void issue_A(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
-                                        StageBars &sb, bool first, int parity_old) {
+__device__ __forceinline__ void issue_C(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
+                                        StageBars &sb, bool first, int prev) {
     constexpr int CHN = Chunk<T>::inner;
     constexpr unsigned HB = halo_bytes<T, CHN>(), HS = halo_slot<T, CHN>(), OB = own_bytes<T, CHN>();
     static_assert(HS % 128 == 0 && OB % 128 == 0, "TMA destinations must be 128-byte aligned");
@@ -545,30 +587,18 @@ __device__ __forceinline__ void issue_A(const DevPtrs &P, int tile, int st, int 
     const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
     unsigned char *B = stage + b * StageSize<T>::buffer();
     const int k0 = st * CHN;
-    mbar_expect_tx(sb.bar + b, (first ? 2 : 3) * HB + OB);
-    tma_halo<T, CHN>((T *)B, maps + MAP_Z_H, td.x0, td.y0, k0, sb.bar + b);
-    if (!first)
-        tma_halo<T, CHN>((T *)(B + HS), maps + (parity_old ? MAP_P1_H : MAP_P0_H), td.x0, td.y0, k0, sb.bar + b);
-    tma_halo<T, CHN>((T *)(B + 2 * HS), maps + MAP_K_H, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<T, CHN>((T *)(B + 3 * HS), maps + MAP_D_O, td.x0, td.y0, k0, sb.bar + b);
-}
-
-template <typename T>
-__device__ __forceinline__ void issue_B(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
-                                        StageBars &sb, bool first, int parity_p) {
-    constexpr int CHN = Chunk<T>::inner;
-    constexpr unsigned OB = own_bytes<T, CHN>();
-    const TileDesc td = P.tiles[tile];
-    const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
-    unsigned char *B = stage + b * StageSize<T>::buffer();
-    const int k0 = st * CHN;
-    mbar_expect_tx(sb.bar + b, (first ? 5 : 6) * OB);
-    tma_own<T, CHN>((T *)B, maps + (parity_p ? MAP_P1_O : MAP_P0_O), td.x0, td.y0, k0, sb.bar + b);
-    tma_own<T, CHN>((T *)(B + OB), maps + MAP_Q_O, td.x0, td.y0, k0, sb.bar + b);
-    if (!first) tma_own<T, CHN>((T *)(B + 2 * OB), maps + MAP_DD_O, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<T, CHN>((T *)(B + 3 * OB), maps + MAP_R_O, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<T, CHN>((T *)(B + 4 * OB), maps + MAP_INV_O, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<T, CHN>((T *)(B + 5 * OB), maps + MAP_C_O, td.x0, td.y0, k0, sb.bar + b);
+    sb.issued(b);
+    mbar_expect_tx(sb.bar + b, (first ? 2 : 4) * HB + (first ? 3 : 4) * OB);
+    tma_halo<T, CHN>((T *)B, maps + (prev ? MAP_Z1_H : MAP_Z0_H), td.x0, td.y0, k0, sb.bar + b);
+    if (!first) {
+        tma_halo<T, CHN>((T *)(B + HS), maps + (prev ? MAP_T1_H : MAP_T0_H), td.x0, td.y0, k0, sb.bar + b);
+        tma_halo<T, CHN>((T *)(B + 2 * HS), maps + (prev ? MAP_P1_H : MAP_P0_H), td.x0, td.y0, k0, sb.bar + b);
+    }
+    tma_halo<T, CHN>((T *)(B + 3 * HS), maps + MAP_K_H, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + 4 * HS), maps + MAP_D_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + 4 * HS + OB), maps + MAP_INV_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<T, CHN>((T *)(B + 4 * HS + 2 * OB), maps + MAP_C_O, td.x0, td.y0, k0, sb.bar + b);
+    if (!first) tma_own<T, CHN>((T *)(B + 4 * HS + 3 * OB), maps + MAP_DD_O, td.x0, td.y0, k0, sb.bar + b);
 }
 
 // Issues chunks 0 and 1 of a tile (the prefetch of the block's next tile).
@@ -580,7 +610,8 @@ __device__ __forceinline__ void issue_head(int nz, Issue issue) {
 // ---- phase R: outer FP64 residual and the preconditioner factors -------------
 // r = b - A x with the FP64 coefficients, r_T = (T) r; the column factors of M
 // (1/den and c') from the inner operator's T coefficients (the same rounding as
-// the stored K, D) are stored; z = M^-1 r_T; v = {||r||^2, ||b||^2, r.z}.
+// the stored K, D) are stored; z = M^-1 r_T into z0 (the inner iteration's
+// "previous" z, buffer 0); v = {||r||^2, ||b||^2, r.z}.
 // Staged: x, K64 (halo), D64, b (own).
 template <typename T, bool DSMEM>
 __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetched, const ColumnRef &cr,
@@ -588,8 +619,7 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
     constexpr int CHN = CH_R;
     typedef Halo<double> H;
     constexpr unsigned HB = halo_slot<double, CHN>(), OB = own_bytes<double, CHN>();
-    T *__restrict__ r = (T *)P.r;
-    T *__restrict__ z = (T *)P.z;
+    T *__restrict__ z = (T *)P.z0;
     T *__restrict__ finv = (T *)P.finv;
     T *__restrict__ fc = (T *)P.fc;
     const size_t BUF = StageSize<T>::buffer();
@@ -634,7 +664,6 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
         v[1] += bk * bk;
         const T rT = (T)rk;
         const long long g = cr.g0 + (long long)k * cr.sxy;
-        r[g] = rT;
         const T Kt = (T)Kc;
         const T kdT = T(mu) * (T(0.5) * (Kt + (T)K_up)), kuT = T(md) * (T(0.5) * (Kt + (T)K_dn));
         const T kwT = T(M.w) * (T(0.5) * (Kt + (T)Kw)), keT = T(M.e) * (T(0.5) * (Kt + (T)Ke));
@@ -659,48 +688,65 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
     if (cr.valid) back_sweep<T, DSMEM>(cr, s_d, fc, z);
 }
 
-// ---- phase A: direction and q = A p ------------------------------------------
-// p_new = z + beta p_old (formed at the lateral neighbours from the staged z and
-// p_old; p is double buffered), q = A p_new, v = {p.q}.
-// Staged: z, p_old, K (halo), D (own).
-template <typename T>
-__device__ void phase_A(const DevPtrs &P, int tile, int tile_next, bool prefetched, bool first_next,
-                        int parity_next, const ColumnRef &cr, const StencilW<T> &w, T beta, bool first,
-                        int parity_old, T *__restrict__ pnew, unsigned char *stage, StageBars &sb,
-                        double (&v)[1]) {
+// ---- inner sweep C: one PCG iteration --------------------------------------
+// With ap = alpha_{i-1} and bt = beta_i (both zero in a cycle's first sweep):
+// z = z_prev - ap t_prev and p = z + bt p_prev at the own column and its four
+// lateral neighbours (from the staged halo boxes) and at k+1; q = A p;
+// t = M^-1 q by the stored factors (forward sweep in the march, back sweep
+// after it); d += ap p_prev.  Writes z, p, t into the buffers other than
+// `prev`, and v = {p.q, z.q, q.t, z.M z}.
+template <typename T, bool DSMEM>
+__device__ void phase_C(const DevPtrs &P, int tile, int tile_next, bool prefetched, bool first_next,
+                        int prev_next, const ColumnRef &cr, const StencilW<T> &w, T ap, T bt, bool first,
+                        int prev, T *s_d, unsigned char *stage, StageBars &sb, double (&v)[4]) {
     constexpr int CHN = Chunk<T>::inner;
     typedef Halo<T> H;
     constexpr unsigned HB = halo_slot<T, CHN>();
-    T *__restrict__ q = (T *)P.q;
+    constexpr int S = CHN * OWN_PLANE;
+    T *__restrict__ z_out = (T *)(prev ? P.z0 : P.z1);
+    T *__restrict__ p_out = (T *)(prev ? P.p0 : P.p1);
+    T *__restrict__ t_out = (T *)(prev ? P.t0 : P.t1);
+    T *__restrict__ d = (T *)P.d;
+    const T *__restrict__ fc = (const T *)P.fc;
     const size_t BUF = StageSize<T>::buffer();
     auto buf = [&](int b) { return stage + b * BUF; };
-    auto issue = [&](int st, int b) { issue_A<T>(P, tile, st, b, stage, sb, first, parity_old); };
+    auto issue = [&](int st, int b) { issue_C<T>(P, tile, st, b, stage, sb, first, prev); };
     auto issue_next = [&]() {
         if (tile_next < P.ntiles)
             issue_head<CHN>(P.dom[P.tiles[tile_next].dom].nz, [&](int st, int b) {
-                issue_A<T>(P, tile_next, st, b, stage, sb, first_next, parity_next);
+                issue_C<T>(P, tile_next, st, b, stage, sb, first_next, prev_next);
             });
     };
     const int nz = cr.nz, hc = H::center(), oc = threadIdx.x;
     const Masks M = masks_of(cr);
     const T mW = (T)M.w, mE = (T)M.e, mS = (T)M.s, mN = (T)M.n;
-    const T bt = first ? T(0) : beta;
-    T p_up = T(0), K_up = T(0);
+    T p_up = T(0), z_up = T(0), K_up = T(0), cprev = T(0), yprev = T(0);
+    // this iteration's z and p at offset o of staged halo planes (z, t, p)
+    auto zv = [&](const T *zz, const T *tt, int o) { return first ? zz[o] : zz[o] - ap * tt[o]; };
+    auto pv = [&](const T *zz, const T *tt, const T *pp, int o) {
+        return first ? zz[o] : (zz[o] - ap * tt[o]) + bt * pp[o];
+    };
     auto plane = [&](int b, int pl, int k) {
         if (!cr.valid) return;
         const T *sz = (const T *)buf(b) + pl * H::PLANE;
-        const T *sq = (const T *)(buf(b) + HB) + pl * H::PLANE;
-        const T *sK = (const T *)(buf(b) + 2 * HB) + pl * H::PLANE;
-        const T *sD = (const T *)(buf(b) + 3 * HB) + pl * OWN_PLANE;
-        auto pv = [&](const T *zz, const T *qq, int o) { return first ? zz[o] : zz[o] + bt * qq[o]; };
-        const T pc = pv(sz, sq, hc);
-        T p_dn = T(0), K_dn = T(0);
+        const T *st = (const T *)(buf(b) + HB) + pl * H::PLANE;
+        const T *sp = (const T *)(buf(b) + 2 * HB) + pl * H::PLANE;
+        const T *sK = (const T *)(buf(b) + 3 * HB) + pl * H::PLANE;
+        const T *own = (const T *)(buf(b) + 4 * HB) + pl * OWN_PLANE + oc;
+        const T Dk = own[0], inv = own[S], cp = own[2 * S];
+        const T zc = zv(sz, st, hc), pc = pv(sz, st, sp, hc);
+        T z_dn = T(0), p_dn = T(0), K_dn = T(0);
         if (k + 1 < nz) {
-            if (pl + 1 < CHN) { p_dn = pv(sz + H::PLANE, sq + H::PLANE, hc); K_dn = sK[H::PLANE + hc]; }
-            else {
-                const T *nz_ = (const T *)buf((b + 1) % STAGES), *nq = (const T *)(buf((b + 1) % STAGES) + HB);
-                p_dn = pv(nz_, nq, hc);
-                K_dn = ((const T *)(buf((b + 1) % STAGES) + 2 * HB))[hc];
+            if (pl + 1 < CHN) {
+                z_dn = zv(sz + H::PLANE, st + H::PLANE, hc);
+                p_dn = pv(sz + H::PLANE, st + H::PLANE, sp + H::PLANE, hc);
+                K_dn = sK[H::PLANE + hc];
+            } else {
+                const unsigned char *nb = buf((b + 1) % STAGES);
+                const T *nzz = (const T *)nb, *ntt = (const T *)(nb + HB), *npp = (const T *)(nb + 2 * HB);
+                z_dn = zv(nzz, ntt, hc);
+                p_dn = pv(nzz, ntt, npp, hc);
+                K_dn = ((const T *)(nb + 3 * HB))[hc];
             }
         }
         const T Kc = sK[hc];
@@ -708,66 +754,35 @@ __device__ void phase_A(const DevPtrs &P, int tile, int tile_next, bool prefetch
         const T kd = mu * (T(0.5) * (Kc + K_up)), ku = md * (T(0.5) * (Kc + K_dn));
         const T kw = mW * (T(0.5) * (Kc + sK[hc - 1])), ke = mE * (T(0.5) * (Kc + sK[hc + 1]));
         const T ks = mS * (T(0.5) * (Kc + sK[hc - H::BW])), kn = mN * (T(0.5) * (Kc + sK[hc + H::BW]));
-        const T Dk = sD[oc];
-        T Ap = Dk * pc + w.cx * (kw * (pc - pv(sz, sq, hc - 1)) + ke * (pc - pv(sz, sq, hc + 1))) +
-               w.cy * (ks * (pc - pv(sz, sq, hc - H::BW)) + kn * (pc - pv(sz, sq, hc + H::BW))) +
-               w.cz * (kd * (pc - p_up) + ku * (pc - p_dn));
-        if (Dk < T(0)) Ap = T(0);  // Dirichlet cell: p is zero there and its row is the identity
-        v[0] += (double)pc * (double)Ap;
+        const bool fixed = Dk < T(0);  // Dirichlet cell: identity row, z = p = 0 there
+        T q = Dk * pc + w.cx * (kw * (pc - pv(sz, st, sp, hc - 1)) + ke * (pc - pv(sz, st, sp, hc + 1))) +
+              w.cy * (ks * (pc - pv(sz, st, sp, hc - H::BW)) + kn * (pc - pv(sz, st, sp, hc + H::BW))) +
+              w.cz * (kd * (pc - p_up) + ku * (pc - p_dn));
+        // (M z)_k with M the column's tridiagonal part of A
+        T Mz = (Dk + w.cx * (kw + ke) + w.cy * (ks + kn)) * zc + w.cz * (kd * (zc - z_up) + ku * (zc - z_dn));
+        if (fixed) {
+            q = T(0);
+            Mz = T(0);
+        }
+        v[0] += (double)pc * (double)q;
+        v[1] += (double)zc * (double)q;
+        v[3] += (double)zc * (double)Mz;
+        const T y = q - cprev * yprev;
+        const T dp = y * inv;
+        v[2] += (double)y * (double)dp;
         const long long g = cr.g0 + (long long)k * cr.sxy;
-        pnew[g] = pc;
-        q[g] = Ap;
+        z_out[g] = zc;
+        p_out[g] = pc;
+        d[g] = first ? T(0) : own[3 * S] + ap * sp[hc];
+        put_dprime<T, DSMEM>(dp, s_d, k, t_out + g);
+        cprev = cp;
+        yprev = y;
         p_up = pc;
+        z_up = zc;
         K_up = Kc;
     };
     march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next);
-}
-
-// ---- phase B: update, residual, preconditioner --------------------------------
-// d += alpha p, r -= alpha q, z = M^-1 r with the stored factors;
-// v = {||r||^2, r.z}.  Column-local: staged p, q, d, r, 1/den, c' (own).
-template <typename T, bool DSMEM>
-__device__ void phase_B(const DevPtrs &P, int tile, int tile_next, bool prefetched, bool first_next,
-                        int parity_next, const ColumnRef &cr, T alpha, bool first, int parity_p, T *s_d,
-                        unsigned char *stage, StageBars &sb, double (&v)[2]) {
-    constexpr int CHN = Chunk<T>::inner;
-    constexpr unsigned OB = own_bytes<T, CHN>();
-    T *__restrict__ r = (T *)P.r;
-    T *__restrict__ z = (T *)P.z;
-    T *__restrict__ d = (T *)P.d;
-    const T *__restrict__ fc = (const T *)P.fc;
-    const size_t BUF = StageSize<T>::buffer();
-    auto buf = [&](int b) { return stage + b * BUF; };
-    auto issue = [&](int st, int b) { issue_B<T>(P, tile, st, b, stage, sb, first, parity_p); };
-    auto issue_next = [&]() {
-        if (tile_next < P.ntiles)
-            issue_head<CHN>(P.dom[P.tiles[tile_next].dom].nz, [&](int st, int b) {
-                issue_B<T>(P, tile_next, st, b, stage, sb, first_next, parity_next);
-            });
-    };
-    const int nz = cr.nz, oc = threadIdx.x;
-    T cprev = T(0), yprev = T(0);
-    auto plane = [&](int b, int pl, int k) {
-        if (!cr.valid) return;
-        const T *B = (const T *)buf(b) + pl * OWN_PLANE + oc;
-        constexpr int S = CHN * OWN_PLANE;
-        const T pc = B[0], qc = B[S], dold = first ? T(0) : B[2 * S], rold = B[3 * S];
-        const T inv = B[4 * S], cp = B[5 * S];
-        const long long g = cr.g0 + (long long)k * cr.sxy;
-        d[g] = dold + alpha * pc;
-        const T rk = rold - alpha * qc;
-        r[g] = rk;
-        v[0] += (double)rk * (double)rk;
-        const T y = rk - cprev * yprev;
-        const T dp = y * inv;
-        put_dprime<T, DSMEM>(dp, s_d, k, z + g);
-        v[1] += (double)y * (double)dp;
-        cprev = cp;
-        yprev = y;
-    };
-    march<CHN, false>(nz, sb, prefetched, issue, plane, issue_next);
-    (void)OB;
-    if (cr.valid) back_sweep<T, DSMEM>(cr, s_d, fc, z);
+    if (cr.valid) back_sweep<T, DSMEM>(cr, s_d, fc, t_out);
 }
 
 __device__ __forceinline__ void finalize_R(const DevPtrs &P, int dom, const double (&v)[3]) {
@@ -792,9 +807,14 @@ __device__ __forceinline__ void finalize_R(const DevPtrs &P, int dom, const doub
         atomicAdd(&P.gctrl->n_inner_active, 1);
         c.inner_iter = 0;
         c.first_inner = 1;
+        c.parity = 0;  // phase R left z in buffer 0
         c.rz = v[2];
+        c.alpha = 0.0;
         c.beta = 0.0;
-        c.inner_target2 = fmax(D.inner_tol * D.inner_tol * rr64, 0.25 * tol2 * bb);
+        // the inner solve reduces r.M^-1 r by inner_tol^2 (mixed mode), or far
+        // enough that ||r|| should meet the outer tolerance (half of it, with
+        // the M^-1-norm standing in for the 2-norm); R checks the true residual
+        c.inner_target2 = v[2] * fmax(D.inner_tol * D.inner_tol, 0.25 * tol2 * bb / rr64);
     }
 }
 
@@ -804,10 +824,11 @@ __device__ __forceinline__ void stop_inner(const DevPtrs &P, KrylovCtrl &c) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 4) k_krylov(DevPtrs P) {
+__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F32 : KRYLOV_BLOCKS_F64)
+    k_krylov(DevPtrs P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar[STAGES];
-    constexpr bool DSMEM = sizeof(T) == 4;
+    constexpr bool DSMEM = sizeof(T) == 4 && KRYLOV_DSMEM_F32;
     // dynamic shared memory: [d' of the column solves (float only)][STAGES
     // staging buffers], the staging buffers 128-byte aligned for the TMA
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -819,7 +840,11 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 4) k_krylov
         mbar_fence_init();
     }
     __syncthreads();
-    StageBars sb{s_bar, 0u, P.barrier};
+    StageBars sb{s_bar, 0u, P.barrier, 0u};
+    // every error exit first lets this block's in-flight stage copies land
+    auto fail = [&]() {
+        if (threadIdx.x == 0) sb.drain();
+    };
     // next tile of this block with an active domain (stride gridDim.x)
     auto next_outer = [&](int t) {
         while (t < P.ntiles && !ldcg(&P.kctrl[P.tiles[t].dom].active)) t += gridDim.x;
@@ -848,98 +873,74 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 4) k_krylov
                 t = tn;
             }
         }
-        if (!grid_sync(P.barrier)) return;
+        if (!grid_sync(P.barrier)) return fail();
         if (ldcg(&P.gctrl->n_active) == 0) break;
-        // ---- inner PCG
+        // ---- inner PCG: one sweep and one grid barrier per iteration
         // A domain's control record (inner_active, parity, first_inner, alpha,
-        // beta) changes only when its last tile of a phase finishes, after
-        // every tile of it in that phase has been scheduled, so within a phase
+        // beta) changes only when its last tile of a sweep finishes, after
+        // every tile of it in that sweep has been scheduled, so within a sweep
         // a block reads it once per domain rather than once per tile.
         struct Ctl {
             int dom, active, parity;
             bool first;
-            double ab;  // beta in phase A, alpha in phase B
+            double alpha, beta;
         };
-        auto ctl_load = [&](Ctl &c, int dom, bool phase_a) {
+        auto ctl_load = [&](Ctl &c, int dom) {
             if (c.dom == dom) return;
             const KrylovCtrl *k = &P.kctrl[dom];
             c.dom = dom;
             c.active = ldcg(&k->inner_active);
             c.parity = ldcg(&k->parity);
             c.first = ldcg(&k->first_inner) != 0;
-            c.ab = phase_a ? ldcg(&k->beta) : ldcg(&k->alpha);
+            c.alpha = ldcg(&k->alpha);
+            c.beta = ldcg(&k->beta);
         };
         // next tile of this block (stride gridDim.x) whose domain iterates
-        auto next_live = [&](Ctl &c, int t, bool phase_a) {
+        auto next_live = [&](Ctl &c, int t) {
             for (; t < P.ntiles; t += gridDim.x) {
                 const int dom = P.tiles[t].dom;
-                if (dom != c.dom) ctl_load(c, dom, phase_a);
+                if (dom != c.dom) ctl_load(c, dom);
                 if (c.active) break;
             }
             return t;
         };
         while (ldcg(&P.gctrl->n_inner_active) > 0) {
             bool pre = false;
-            Ctl cc{-1, 0, 0, false, 0.0}, cn{-1, 0, 0, false, 0.0};
-            for (int t = next_live(cc, blockIdx.x, true); t < P.ntiles;) {
-                const int tn = next_live(cn, t + gridDim.x, true);
+            Ctl cc{-1, 0, 0, false, 0.0, 0.0}, cn{-1, 0, 0, false, 0.0, 0.0};
+            for (int t = next_live(cc, blockIdx.x); t < P.ntiles;) {
+                const int tn = next_live(cn, t + gridDim.x);
                 const int dom = P.tiles[t].dom;
-                ctl_load(cc, dom, true);
-                const ColumnRef cr = column_of(P, t);
-                const int parity = cc.parity;
-                const bool first = cc.first;
-                const T beta = (T)cc.ab;
-                const bool first_n = tn < P.ntiles ? cn.first : false;
-                const int parity_n = tn < P.ntiles ? cn.parity : 0;
-                T *pnew = (T *)(parity ? P.p0 : P.p1);
-                double v[1] = {0.0};
-                phase_A<T>(P, t, tn, pre, first_n, parity_n, cr, weights(dom), beta, first, parity, pnew,
-                           stage_raw, sb, v);
-                pre = tn < P.ntiles;
-                if (domain_reduce<1>(P, t, dom, 0, v) && threadIdx.x == 0) {
-                    KrylovCtrl &c = P.kctrl[dom];
-                    c.alpha = c.rz / v[0];
-                    c.parity ^= 1;
-                    if (!(v[0] > 0.0) || isinf(v[0])) stop_inner(P, c);
-                }
-                t = tn;
-            }
-            if (!grid_sync(P.barrier)) return;
-            pre = false;
-            cc = Ctl{-1, 0, 0, false, 0.0};
-            cn = Ctl{-1, 0, 0, false, 0.0};
-            for (int t = next_live(cc, blockIdx.x, false); t < P.ntiles;) {
-                const int tn = next_live(cn, t + gridDim.x, false);
-                const int dom = P.tiles[t].dom;
-                ctl_load(cc, dom, false);
+                ctl_load(cc, dom);
                 const ColumnRef cr = column_of(P, t);
                 const DomainDesc &D = P.dom[dom];
-                const int parity = cc.parity;
-                const bool first = cc.first;
-                const T alpha = (T)cc.ab;
                 const bool first_n = tn < P.ntiles ? cn.first : false;
-                const int parity_n = tn < P.ntiles ? cn.parity : 0;
-                double v[2] = {0.0, 0.0};
-                phase_B<T, DSMEM>(P, t, tn, pre, first_n, parity_n, cr, alpha, first, parity, s_d, stage_raw,
-                                  sb, v);
+                const int prev_n = tn < P.ntiles ? cn.parity : 0;
+                double v[4] = {0.0, 0.0, 0.0, 0.0};
+                phase_C<T, DSMEM>(P, t, tn, pre, first_n, prev_n, cr, weights(dom), (T)cc.alpha, (T)cc.beta,
+                                  cc.first, cc.parity, s_d, stage_raw, sb, v);
                 pre = tn < P.ntiles;
-                if (domain_reduce<2>(P, t, dom, 0, v) && threadIdx.x == 0) {
+                if (domain_reduce<4>(P, t, dom, 0, v) && threadIdx.x == 0) {
                     KrylovCtrl &c = P.kctrl[dom];
-                    c.rr = v[0];
-                    c.beta = v[1] / c.rz;
-                    c.rz = v[1];
+                    const double sigma = v[0], mu = v[1], nu = v[2], rho = v[3];
+                    const double alpha = rho / sigma;
+                    const double rho_next = rho - 2.0 * alpha * mu + alpha * alpha * nu;
+                    const bool bad = !(sigma > 0.0) || isinf(sigma) || !(rho > 0.0) || !(rho_next == rho_next);
+                    c.alpha = bad ? 0.0 : alpha;  // a broken iteration leaves x alone
+                    c.beta = bad ? 0.0 : rho_next / rho;
+                    c.rz = rho_next;
+                    c.parity ^= 1;
                     c.first_inner = 0;
                     c.inner_iter += 1;
                     c.total_iter += 1;
-                    if (v[0] <= c.inner_target2 || c.inner_iter >= D.inner_maxiter ||
-                        c.total_iter >= D.krylov_maxiter || !(v[0] == v[0]) || !(v[1] == v[1]))
+                    if (bad || rho_next <= c.inner_target2 || c.inner_iter >= D.inner_maxiter ||
+                        c.total_iter >= D.krylov_maxiter)
                         stop_inner(P, c);
                 }
                 t = tn;
             }
-            if (!grid_sync(P.barrier)) return;
+            if (!grid_sync(P.barrier)) return fail();
         }
-        // ---- U: x += d
+        // ---- U: x += d + alpha p (the last iteration's pending update)
         for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
             const int dom = P.tiles[t].dom;
             const KrylovCtrl *kc = &P.kctrl[dom];
@@ -947,14 +948,16 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? 5 : 4) k_krylov
             const ColumnRef cr = column_of(P, t);
             if (!cr.valid) continue;
             const T *__restrict__ d = (const T *)P.d;
+            const T *__restrict__ p = (const T *)(ldcg(&kc->parity) ? P.p1 : P.p0);
+            const double a = ldcg(&kc->alpha);
             double *__restrict__ x = P.x;
 #pragma unroll 8
             for (int k = 0; k < cr.nz; ++k) {
                 const long long g = cr.g0 + (long long)k * cr.sxy;
-                x[g] += (double)d[g];
+                x[g] += (double)d[g] + a * (double)p[g];
             }
         }
-        if (!grid_sync(P.barrier)) return;
+        if (!grid_sync(P.barrier)) return fail();
     }
 }
 
@@ -1029,6 +1032,8 @@ __global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
     // v: 0 sum dtheta*dz, 1 dt*sum ssflux, 2 sum transp, 3 dt*boundary flux,
     //    4 storage (telescoping), 5 dt*q_top, 6 dt*q_bottom, 7 rain, 8 nonfinite
     double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long bsig = 0;
+    const int step_now = P.pctrl[td.dom].step;
     if (cr.valid) {
         const double dt = D.dt, dz = D.dz;
         const double ssc = D.Ss / dt / D.porosity;
@@ -1054,6 +1059,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
             else if (upd == DHARA_THETA_CONSERVATIVE) th_next = thm + Cm * (xn - xm);
             else th_next = thm;
             v[4] += dz * (th_next - thn) + dz * ssc * dt * thm * (xn - psin);
+            if (D.record_branches) bsig += branch_mix(step_now * 64 + 63, BR_SATURATION, g, band3(xn, 0.0, 1e-9));
             if (!(xn == xn)) v[8] = 1.0;
             // boundary faces (Neumann values; bottom/top below)
             double fb = 0.0;
@@ -1079,7 +1085,11 @@ __global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
         const double ph = fmax(P.hpoten[cr.c] - qt * dt, 0.0);
         P.ph[cr.c] = ph;
         P.h[cr.c] = ph;
+        if (D.record_branches)
+            bsig += branch_mix(step_now, BR_PONDCLIP, cr.c,
+                               band3(P.hpoten[cr.c], qt * dt, rel_band(P.hpoten[cr.c], qt * dt, 1e-15)));
     }
+    if (D.record_branches) branch_commit(&P.diag[td.dom].branch_sig, bsig);
     if (domain_reduce<9>(P, tile, td.dom, 2, v) && threadIdx.x == 0) {
         DevDiag &dg = P.diag[td.dom];
         PicardCtrl &pc = P.pctrl[td.dom];
@@ -1094,6 +1104,8 @@ __global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
         dg.picard_iters_total += pc.iter;
         dg.picard_iters_last = pc.iter;
         if (!pc.converged) dg.picard_nonconverged += 1;
+        if (D.record_branches)
+            atomicAdd(&dg.branch_sig, branch_mix(pc.step, BR_PICARD, td.dom, (unsigned)pc.iter));
         pc.step += 1;
     }
 }
@@ -1181,7 +1193,7 @@ cudaError_t configure_3d(LaunchCfg &L, int device, int ntiles) {
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e != cudaSuccess) return e;
     const size_t elt = L.mixed ? sizeof(float) : sizeof(double);
-    const size_t dprime = L.mixed ? elt * (size_t)L.nz_max * TILE_THREADS : 0;
+    const size_t dprime = (L.mixed && KRYLOV_DSMEM_F32) ? elt * (size_t)L.nz_max * TILE_THREADS : 0;
     const size_t stage = L.mixed ? StageSize<float>::bytes() : StageSize<double>::bytes();
     L.smem_3d = (int)(128 + ((dprime + 127) & ~(size_t)127) + stage);
     const void *fn = L.mixed ? (const void *)k_krylov<float> : (const void *)k_krylov<double>;

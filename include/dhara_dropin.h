@@ -34,6 +34,42 @@
 
 #include "dhara_gpu.h"
 
+#ifndef PROJECTCLASS_H
+#define PROJECTCLASS_H
+/* include/class.h:3-33: the output settings SaveModelResults and
+ * SaveResultEntirePeriod read (SAVE_*, OUTPUT_* keys, src/io.cc:466-493). */
+class ProjectClass {
+  public:
+    const char *name;
+    const char *folderoutput;
+    const char *mlcanoutput;
+    const char *olfoutput;
+    const char *ssfoutput;
+    const char *ssf1doutput;
+    const char *statoutput;
+
+    int co2elevation;
+    int numberofplants;
+    int planttype;
+    int savemlcan;
+    int saveolf;
+    int savessf;
+    int savestat;
+    int saveinterval;
+    int printiterval;
+    int num_steps;
+
+    int verbose;
+    int version;
+
+    double co2concentration;
+    double dtimehr;
+    double dx_meter;
+    double dy_meter;
+    double dz_meter;
+};
+#endif
+
 #ifndef TIMEFORCINGCLASS_H
 #define TIMEFORCINGCLASS_H
 class TimeForcingClass {
@@ -187,5 +223,22 @@ void SubsurfaceFlowModel(TimeForcingClass *&timeforcings, OverlandFlowClass *&ov
 void OverlandFlowModel(TimeForcingClass *&timeforcings, OverlandFlowClass *&overland_dev,
                        SubsurfaceFlowClass *&subsurface_dev, dhara_handle *solver, int rank, int procsize,
                        int3 globsize, int t, int num_steps);
+
+/* SaveModelResults (src/io.cc:854-906): every saveinterval steps, copies
+ * waterelev/waterdepth (when saveolf) and psin/thetan (when savessf) from the
+ * device structs into the host structs' arrays (waterelev, waterdepth,
+ * psiout, thetaout) and writes <folderoutput>/<olfoutput>_<timestep>.nc and
+ * <folderoutput>/<ssfoutput>_<timestep>.nc with the reference's variables
+ * (dhara_write_netcdf_state). */
+void SaveModelResults(ProjectClass *project, OverlandFlowClass *overland_host, OverlandFlowClass *overland_dev,
+                      SubsurfaceFlowClass *subsurface_host, SubsurfaceFlowClass *subsurface_dev, int3 globsize,
+                      int timestep);
+
+/* The flow-model part of SaveResultEntirePeriod (src/io.cc:962-996; the
+ * MLCan part and its MPI arguments are out of scope): when savestat, writes
+ * <folderoutput>/<ssf1doutput>.nc (mb_subsurfaceW over num_steps) and
+ * <folderoutput>/<statoutput>.nc (psi_col, theta_col as pressure_mean,
+ * moisture_mean [num_steps][nz]) from the host struct. */
+void SaveResultEntirePeriod(ProjectClass *project, SubsurfaceFlowClass *subsurface_host, int3 globsize);
 
 #endif

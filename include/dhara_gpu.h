@@ -105,7 +105,10 @@ typedef struct {
      * the FP64 system's); 1 evaluates the closure in FP32 (faster; the
      * refinement then converges to the FP32-coefficient system). */
     int32_t closure_fp32;
-    int32_t reserved_i[6];
+    /* 1: accumulate dhara_diagnostics.branch_signature (costs a hash and a
+     * warp-aggregated atomic per decision; off by default). */
+    int32_t record_branches;
+    int32_t reserved_i[5];
     double reserved_d[8];
 } dhara_params;
 
@@ -177,7 +180,21 @@ typedef struct {
     double ponded_volume;           /* sum h over columns after the last step, m */
     double picard_err_last;         /* last Picard difference measure */
     double krylov_relres_last;      /* last ||r||/||b|| of the 3D solve */
-    double reserved[6];
+    /* With record_branches: an order-independent 64-bit hash-sum over every
+     * discrete decision of the run -- the top-flux selection per column and
+     * step (src/global.cu:236-251), the ponding clip (src/subsurface.cu:480),
+     * saturation (psi >= 0) of every cell at every closure evaluation
+     * (src/global.cu:79-97), Manning's wet/slope test per face
+     * (src/overland.cu:279-297), the overland depth clip
+     * (src/overland.cu:378) and the Picard iteration count.  Each comparison
+     * is recorded as below / on / above its boundary, "on" meaning within a
+     * rounding band (1e-9 relative, or 1e-9 m / 1e-9 for depths, heads and
+     * slopes), so a comparison that ties up to rounding records the same in
+     * every run.  Two runs with equal signatures took the same branches
+     * everywhere, so a finite difference between them differentiates one
+     * smooth piece.  0 when not recorded. */
+    uint64_t branch_signature;
+    double reserved[5];
 } dhara_diagnostics;
 
 /* ---- lifetime ---------------------------------------------------------- */
@@ -297,6 +314,30 @@ int dhara_snapshot(dhara_handle *h, int domain, double *water_elevation, double 
                    double *pressure_head, double *moisture);
 int dhara_snapshot_wait(dhara_handle *h);
 
+/* ---- NetCDF result files -----------------------------------------------------
+ * The reference's output files (SaveModelResults, src/io.cc:854-906, and the
+ * flow-model part of SaveResultEntirePeriod, src/io.cc:962-996, through its
+ * SaveOutput1D/2D/3D, src/io.cc:696-850) in NetCDF classic format, written by
+ * the library (no netCDF library needed); 64-bit-offset format when a file
+ * exceeds 2 GiB.  Variables and dimensions as the reference defines them:
+ *   file2d: water_elevation, water_depth   [ny][nx], dimensions named "x", "y"
+ *           (SaveOutput2D's names: "x" is the slower dimension)
+ *   file3d: pressure_head, moisture        [nz][ny][nx], dimensions "z", "y", "x"
+ *   file1d: mb_subsurfaceW                 [nsteps], dimension "time_series"
+ *   file_stat: pressure_mean, moisture_mean [nsteps][nz], dimensions "x", "y"
+ *           (CopyLayers' per-layer sums, src/device.cu:135-147)
+ * Any file argument may be NULL (not written).  The writers take host
+ * arrays in the reference layout; the dhara_save_* forms take them from a
+ * handle (the current state, and the statistics of dhara_enable_statistics). */
+int dhara_write_netcdf_state(const char *file2d, const char *file3d, int nx, int ny, int nz,
+                             const double *water_elevation, const double *water_depth,
+                             const double *pressure_head, const double *moisture);
+int dhara_write_netcdf_statistics(const char *file1d, const char *file_stat, int nsteps, int nz,
+                                  const double *mb_subsurfaceW, const double *pressure_sum,
+                                  const double *moisture_sum);
+int dhara_save_netcdf_state(dhara_handle *h, int domain, const char *file2d, const char *file3d);
+int dhara_save_netcdf_statistics(dhara_handle *h, int domain, const char *file1d, const char *file_stat);
+
 /* ---- checkpoint and restart -------------------------------------------------
  * The reference has no restart path (it runs one time loop from the initial
  * condition, src/device.cu:374-475); these save and restore the state a step
@@ -395,9 +436,9 @@ int dhara_adjoint(dhara_handle *h, const dhara_adjoint_desc *desc, double *loss,
 
 /* ---- allocation-free overland step ---------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
- * memory when they step (a host model that owns every GPU buffer, code
- * running during CUDA stream capture, a loop that forbids allocation after
- * start-up): one overland step of one domain -- the computation of
+ * memory when they step (a host model that owns every GPU buffer and leaves
+ * none spare, a loop that forbids allocation after start-up): one overland
+ * step of one domain -- the computation of
  * dhara_overland_step -- on the caller's device arrays.  waterdepth is read
  * as the depth before the step and overwritten with the depth after it;
  * waterelev receives H = h + z after the solve; ztopo and mann are read.
@@ -407,8 +448,12 @@ int dhara_adjoint(dhara_handle *h, const dhara_adjoint_desc *desc, double *loss,
  * that every GPU loading the library keeps until exit; larger domains return
  * DHARA_ERR_UNSUPPORTED.  Calls share that array: calls whose GPU work
  * overlaps race, so order them on one stream.  The first call on a device
- * looks up the array's address (cudaGetSymbolAddress); make it before any
- * stream capture.  Nothing is allocated, nothing is synchronised. */
+ * looks up the array's address (cudaGetSymbolAddress) and keeps it for the
+ * life of the process; make it before any stream capture, and do not call
+ * again on a device after cudaDeviceReset.  waterdepth and waterelev must not
+ * overlap each other, ztopo or mann (DHARA_ERR_INVALID).  Convergence is not
+ * reported: the solve stops at overland_tol or overland_maxiter and returns
+ * DHARA_OK either way.  Nothing is allocated, nothing is synchronised. */
 #define DHARA_NOALLOC_MAX_COLUMNS 16384
 int dhara_overland_step_noalloc(const dhara_params *p, double *waterdepth, const double *ztopo,
                                 const double *mann, double *waterelev, void *stream);

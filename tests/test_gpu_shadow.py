@@ -9,9 +9,16 @@ overland water elevation H:
 
   32x32x20 workload, all 60 steps ........... FP64 1e-8, mixed 1e-4
   64x64x40 patch of the 512x512x40 storm,
-    all 240 steps (mixed) / first 60 (FP64) . mixed 1e-4, FP64 1e-8
+    all 240 steps (mixed) / first 60 (FP64) . mixed 1e-4, FP64 1e-7
 
-Norm-wise relative errors max|gpu - oracle| / max|oracle|.  Free-running
+Norm-wise relative errors max|gpu - oracle| / max|oracle|.  The ponded depth
+is a small difference H - z whose error is set by the overland solve's
+tolerance (1e-12 of ||H||), so its FP64 bound is the 1e-6 of the FP64
+target.  On the storm patch every step runs ten Picard iterations that do not
+converge (the reference scheme on that physics, in the oracle as here); one
+such step amplifies the 1e-12 differences of two converged linear solvers
+~1e4-fold (the oracle against itself with BiCGSTAB instead of CG: 3.5e-9
+after one step), hence 1e-7 there in FP64.  Free-running
 trajectories drift further apart than any one step (the scheme's discrete
 switches amplify rounding; tests/test_oracle_drift.py shows the oracle doing
 the same against itself), so the free-running GPU-vs-oracle difference is
@@ -49,7 +56,7 @@ def test_shadow_32x32x20_all_60_steps(gpu, prec, tol):
     s = solver_for(d)
     r = sh.shadow(s, d, 60)
     s.close()
-    check(r, tol)
+    check(r, tol, tol_ponding=max(tol, 1e-6))
     if prec == db.FP64:
         assert r["picard_mismatch_steps"] == []
 
@@ -72,7 +79,7 @@ def test_shadow_storm_patch_fp64(gpu):
     s = solver_for(d)
     r = sh.shadow(s, d, 60)
     s.close()
-    check(r, 1e-8)
+    check(r, 1e-7, tol_ponding=1e-6)
 
 
 def test_free_run_drift_within_the_oracles_own_spread(gpu):

@@ -2,12 +2,12 @@
 
 It exists for callers that cannot allocate device memory when they step --
 a host model that owns every GPU buffer and hands the library only its own
-arrays, code running while a CUDA stream is captured into a graph, a loop
-that forbids allocation after start-up.  This test calls it through the C
-ABI on device arrays the test owns and checks it against the handle-based
-dhara_overland_step on the same inputs, for two calls in a row (the second
-starting from the first one's output), at the tolerances of the other GPU
-parity tests.  It lives in its own file, collected last, and passes alone in
+arrays, a loop that forbids allocation after start-up.  This test calls it
+through the C ABI on device arrays the test owns and checks it against the
+handle-based dhara_overland_step on the same inputs, for two calls in a row
+(the second starting from the first one's output), at the tolerances of the
+other GPU parity tests, on a small surface and on one at the 16,384-column
+limit of the fixed scratch array.  It lives in its own file, collected last, and passes alone in
 a fresh process as well as after the other tests.
 """
 import ctypes as ct
@@ -38,9 +38,10 @@ def _ponded_domain(nx=48, ny=40, seed=21):
     return d, h
 
 
-def test_noalloc_matches_handle_path_two_calls(gpu):
+@pytest.mark.parametrize("nx,ny", [(48, 40), (128, 128)])
+def test_noalloc_matches_handle_path_two_calls(gpu, nx, ny):
     import torch
-    d, h0 = _ponded_domain()
+    d, h0 = _ponded_domain(nx, ny)
     p = d.params
     # the existing entry point: a handle, two overland steps
     s = db.Solver(p)
@@ -80,3 +81,18 @@ def test_noalloc_rejects_oversize(gpu):
     rc = _noalloc()(ct.byref(p), buf.data_ptr(), buf.data_ptr(), buf.data_ptr(), buf.data_ptr(), None)
     assert rc == 4
     assert "exceeds" in db.lib().dhara_last_error().decode()
+
+
+def test_noalloc_rejects_overlapping_arrays(gpu):
+    import torch
+    d, _ = _ponded_domain()
+    p = d.params
+    C = p.nx * p.ny
+    dev = torch.device("cuda", 0)
+    buf = torch.zeros(3 * C, dtype=torch.float64, device=dev)
+    base = buf.data_ptr()
+    fn = _noalloc()
+    # waterelev overlapping waterdepth (shifted by one cell)
+    rc = fn(ct.byref(p), base, base + 2 * C * 8, base + 2 * C * 8, base + 8, None)
+    assert rc == 1
+    assert "overlap" in db.lib().dhara_last_error().decode()
