@@ -215,7 +215,7 @@ def run_ours(args, world, rank, local):
     def fresh_tuned(precision=db.MIXED):
         s_ = fresh(precision)
         s_.set_launch_config(launch_cfg["krylov_blocks_per_sm"], launch_cfg["overland_resident"],
-                             launch_cfg["overland_blocks_per_sm"])
+                             launch_cfg["overland_blocks_per_sm"], launch_cfg["tile_shape"])
         return s_
 
     s = fresh_tuned()
@@ -364,7 +364,7 @@ def run_ensemble(args, local, world=1, rank=0):
     if args.warmup > 0:
         ens.run_sharded(doms, args.warmup, rank, world, device=local)
     barrier(world)
-    ms, launches, diags = ens.run_sharded(doms, nsteps, rank, world, device=local)
+    ms, launches, diags = ens.run_sharded(doms, nsteps, rank, world, device=local, autotune=2 if args.autotune else 0)
     ms_max = max_over_ranks(ms, world)
     worst_mass = 0.0
     kry_nc = olf_nc = solves = 0
@@ -385,6 +385,8 @@ def run_ensemble(args, local, world=1, rank=0):
             "scaling": "strong" if world > 1 else None,
             "shard_balance": ens.balance([d.ncells for d in doms], world),
             "gpu_launches": launches, "gpu_launches_note": "this rank's" if world > 1 else None,
+            "launches_per_step": launches / nsteps if nsteps else None,
+            "launch_config": diags[0].get("launch_config"),
             "worst_mass_error_over_inflow": worst_mass, "subsurface_solves": solves,
             "subsurface_solves_at_cap": kry_nc, "overland_solves_at_cap": olf_nc,
             "picard_steps_at_cap": sum(diags[i]["picard_nonconverged"] for i in range(len(doms))),
@@ -489,7 +491,10 @@ def fd_check(dom, th_t, q_t, nsteps, local, ncells=32, steps=(1e-4, 1e-5, 1e-6))
     from dhara_b200 import inputs
     p = type(dom.params).from_buffer_copy(dom.params)
     p.precision = db.FP64
-    p.record_branches = 1
+    # the loss's switches (not saturation: theta and K are continuous there) and the
+    # overland iteration counts (a CG stopped at another iteration is another map)
+    p.record_branches = 1 | 2 | 4 | 8 | 32 | 64
+    p.krylov_tol, p.krylov_maxiter, p.overland_tol, p.overland_maxiter = 1e-13, 5000, 1e-12, 50000
     d = inputs.Domain(params=p, fields=dom.fields, int_fields=dom.int_fields, rain_mm=dom.rain_mm)
     th, q = th_t[:nsteps], q_t[:nsteps]
 
@@ -504,7 +509,7 @@ def fd_check(dom, th_t, q_t, nsteps, local, ncells=32, steps=(1e-4, 1e-5, 1e-6))
 
     (L, g_lk, g_al, g_n), base = run(d, True)
     rng = np.random.default_rng(2024)
-    out = {"steps": nsteps, "precision": "fp64", "h_tried": list(steps),
+    out = {"steps": nsteps, "precision": "fp64", "solves": "3D 1e-13, overland 1e-12", "h_tried": list(steps),
            "rule": "accepted h: +h and -h runs keep every branch of the unperturbed run; "
                    "error relative to |fd| where |fd| >= 1e-3 max|g|, else relative to max|g|"}
     for name, g, field, n in (("log_ks", g_lk, "ksat", ncells), ("alpha", g_al, "alpha", 8), ("n", g_n, "nvg", 8)):

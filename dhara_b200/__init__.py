@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdhara_b200.so")
 
 KERNELS = {"krylov": 0, "assemble": 1, "picard_check": 2, "epilogue": 3, "overland_solve": 4,
-           "overland_aux": 5, "prologue": 6, "adjoint": 7}
+           "overland_aux": 5, "prologue": 6, "adjoint": 7, "step": 8}
 
 _lib = None
 
@@ -190,10 +190,16 @@ class Solver:
         _check(lib().dhara_get_launch_config(self.h, ct.byref(c)))
         return c.as_dict()
 
-    def set_launch_config(self, krylov_blocks_per_sm, overland_resident, overland_blocks_per_sm):
+    def set_launch_config(self, krylov_blocks_per_sm, overland_resident, overland_blocks_per_sm, tile_shape=None,
+                          fused_step=None):
+        """Sets the block schedule; tile_shape 0 (per domain), 1 (32 x 4) or 2
+        (16 x 8), fused_step 0/1; None keeps the current value."""
+        cur = self.launch_config()
         c = _abi.LaunchConfig()
         c.krylov_blocks_per_sm, c.overland_resident = krylov_blocks_per_sm, overland_resident
         c.overland_blocks_per_sm = overland_blocks_per_sm
+        c.tile_shape = cur["tile_shape"] if tile_shape is None else tile_shape
+        c.fused_step = cur["fused_step"] if fused_step is None else fused_step
         _check(lib().dhara_set_launch_config(self.h, ct.byref(c)))
 
     def enable_statistics(self, max_steps):

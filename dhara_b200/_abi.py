@@ -74,8 +74,9 @@ class Diagnostics(ct.Structure):
 
 class LaunchConfig(ct.Structure):
     _fields_ = [("krylov_blocks_per_sm", ct.c_int32), ("overland_resident", ct.c_int32),
-                ("overland_blocks_per_sm", ct.c_int32), ("pad", ct.c_int32),
-                ("krylov_ms", ct.c_double), ("overland_ms", ct.c_double)]
+                ("overland_blocks_per_sm", ct.c_int32), ("tile_shape", ct.c_int32),
+                ("krylov_ms", ct.c_double), ("overland_ms", ct.c_double), ("fused_step", ct.c_int32),
+                ("pad", ct.c_int32)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n != "pad"}

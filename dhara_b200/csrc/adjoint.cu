@@ -325,6 +325,8 @@ __global__ void __launch_bounds__(TILE_THREADS) k_adj_matrix(DevPtrs P, AdjPtrs 
         kc.total_iter = 0;
         kc.parity = 0;
         kc.first_inner = 1;
+        kc.keep_p = 0;
+        kc.rho_last = 0.0;
         atomicAdd(&P.gctrl->n_active, 1);
     }
     const ColumnRef cr = column_of(P, tile);

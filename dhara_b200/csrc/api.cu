@@ -40,7 +40,7 @@ int fail(int code, const char *fmt, ...) {
             return fail(DHARA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
     } while (0)
 
-enum { KT_KRYLOV = 0, KT_ASSEMBLE, KT_CHECK, KT_EPILOGUE, KT_OLF_SOLVE, KT_OLF_AUX, KT_PROLOGUE, KT_ADJOINT, KT_N };
+enum { KT_KRYLOV = 0, KT_ASSEMBLE, KT_CHECK, KT_EPILOGUE, KT_OLF_SOLVE, KT_OLF_AUX, KT_PROLOGUE, KT_ADJOINT, KT_STEP, KT_N };
 
 }  // namespace
 
@@ -54,6 +54,8 @@ struct dhara_handle {
     std::vector<dhara_params> params;
     std::vector<DomainDesc> hdom;
     std::vector<TileDesc> htiles;
+    int tile_mode = 0;      // dhara_launch_config::tile_shape in effect
+    size_t tiles_cap = 0;   // capacity of the device tile list and per-tile partials
     std::vector<OlfSeg> hsegs;
     long long Ntot = 0, Ctot = 0, WEtot = 0, SNtot = 0;
     DevPtrs P{};
@@ -69,6 +71,7 @@ struct dhara_handle {
     // graph replay
     cudaGraphExec_t graph_exec = nullptr;
     bool graph_failed = false;
+    long long graph_launches = 0;  // kernels in the captured step
     // timing
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[KT_N];
@@ -199,10 +202,19 @@ void collect_timing(dhara_handle *h) {
     } while (0)
 
 // With a tape (the adjoint's recompute sweep), every Picard iterate psi^m and
-// solution x^m is copied into the tape slot after its solve.
+// solution x^m is copied into the tape slot after its solve, so the step runs
+// as separate launches; otherwise, with the fused schedule, as one k_step.
 int enqueue_subsurface(dhara_handle *h, const AdjPtrs *tape = nullptr, int slot = 0) {
     const DevPtrs &P = h->P;
     cudaStream_t s = h->stream;
+    if (!tape && h->L.fused_step) {
+        LAUNCH(KT_STEP, launch_step(P, h->L, h->maxiter_picard, h->any_dirichlet ? 1 : 0, s));
+        if (h->stats_steps > 0) {
+            LAUNCH(KT_EPILOGUE, launch_layer_stats(P, h->stats_part, h->nz_max, h->stats_hist, h->stats_steps, s));
+            h->launch_count += 1;  // the statistics are two kernels
+        }
+        return DHARA_OK;
+    }
     LAUNCH(KT_PROLOGUE, launch_prologue(P, s));
     for (int m = 0; m < h->maxiter_picard; ++m) {
         LAUNCH(KT_ASSEMBLE, launch_assemble(P, h->L, s));
@@ -312,6 +324,54 @@ int upload_dom_desc(dhara_handle *h) {
     return DHARA_OK;
 }
 
+// Tiles of a domain with shape tx x ty.
+size_t tile_count(const DomainDesc &D, int tx, int ty) {
+    return (size_t)((D.nx + tx - 1) / tx) * (size_t)((D.ny + ty - 1) / ty);
+}
+
+// Tile shape of each domain and the tile list for `mode` (dhara_launch_config
+// tile_shape): 1 all 32 x 4, 2 all 16 x 8, 0 per domain the shape with fewer
+// tiles (fewer idle threads in ragged tiles; 32 x 4 on a tie, its rows being
+// whole 128-byte lines).  Tiles of a domain are consecutive, row by row.
+void plan_tiles(dhara_handle *h, int mode) {
+    h->htiles.clear();
+    for (int d = 0; d < h->ndom; ++d) {
+        DomainDesc &D = h->hdom[d];
+        bool narrow = mode == 2;
+        if (mode == 0) narrow = tile_count(D, 16, 8) < tile_count(D, TILE_X, TILE_Y);
+        D.tx = narrow ? 16 : TILE_X;
+        D.ty = narrow ? 8 : TILE_Y;
+        D.tx_log2 = narrow ? 4 : 5;
+        D.tile_begin = (int)h->htiles.size();
+        for (int y0 = 0; y0 < D.ny; y0 += D.ty)
+            for (int x0 = 0; x0 < D.nx; x0 += D.tx) h->htiles.push_back({d, x0, y0, 0});
+        D.tile_end = (int)h->htiles.size();
+    }
+    h->tile_mode = mode;
+    h->L.uniform_tx = h->hdom[0].tx;
+    for (const DomainDesc &D : h->hdom)
+        if (D.tx != h->L.uniform_tx) h->L.uniform_tx = 0;
+}
+
+int build_tensor_maps(dhara_handle *h);
+
+// Uploads the tile list and the domain table of the current plan and re-encodes
+// the TMA boxes (their extents are the tile shape's); any captured step graph
+// holds the old grid sizes and is dropped.
+int apply_tiles(dhara_handle *h) {
+    if (h->htiles.size() > h->tiles_cap) return fail(DHARA_ERR_INVALID, "internal: tile list exceeds capacity");
+    CK(cudaMemcpyAsync((void *)h->P.tiles, h->htiles.data(), sizeof(TileDesc) * h->htiles.size(),
+                       cudaMemcpyHostToDevice, h->stream));
+    h->P.ntiles = (int)h->htiles.size();
+    int rc = upload_dom_desc(h);
+    if (!rc) rc = build_tensor_maps(h);
+    if (h->graph_exec) {
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    return rc;
+}
+
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against libcuda).
@@ -331,16 +391,17 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // One 3D tiled map over a domain's part of a pitched array: dims (nx, ny, nz),
-// row pitch nxp; box (TILE_X + 2*xoff, TILE_Y + 2, chunk) for halo reads or
-// (TILE_X, TILE_Y, chunk) for own-column reads.  Out-of-range elements read as
-// zero.
+// row pitch nxp; box (tx + 2*xoff, ty + 2, chunk) for halo reads or
+// (tx, ty, chunk) for own-column reads, tx x ty the domain's tile shape.
+// Out-of-range elements read as zero.
 int encode_map(CUtensorMap *m, const void *array, size_t elt, const DomainDesc &D, bool halo, int chunk) {
+    const int TX = D.tx, TY = D.ty;
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return fail(DHARA_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
     const cuuint64_t dims[3] = {(cuuint64_t)D.nx, (cuuint64_t)D.ny, (cuuint64_t)D.nz};
     const cuuint64_t strides[2] = {(cuuint64_t)D.nxp * elt, (cuuint64_t)D.nxp * D.ny * elt};
     const int xoff = (int)(16 / elt);
-    const cuuint32_t box[3] = {(cuuint32_t)(halo ? TILE_X + 2 * xoff : TILE_X), (cuuint32_t)(halo ? TILE_Y + 2 : TILE_Y),
+    const cuuint32_t box[3] = {(cuuint32_t)(halo ? TX + 2 * xoff : TX), (cuuint32_t)(halo ? TY + 2 : TY),
                                (cuuint32_t)chunk};
     const cuuint32_t estr[3] = {1, 1, 1};
     void *base = (void *)((const char *)array + (size_t)D.off3 * elt);
@@ -379,8 +440,8 @@ int build_tensor_maps(dhara_handle *h) {
         rc |= encode_map(m + MAP_B_O, P.b, 8, D, false, CH_R);
         if (rc) return rc;
     }
-    CUtensorMap *dm = nullptr;
-    if (dalloc(h, &dm, maps.size())) return DHARA_ERR_NOMEM;
+    CUtensorMap *dm = const_cast<CUtensorMap *>(h->P.tmaps);
+    if (!dm && dalloc(h, &dm, maps.size())) return DHARA_ERR_NOMEM;
     CK(cudaMemcpyAsync(dm, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     h->P.tmaps = dm;
@@ -407,7 +468,7 @@ int dhara_enable_statistics(dhara_handle *h, int max_steps) {
     if (set_dev(h)) return DHARA_ERR_CUDA;
     CK(cudaStreamSynchronize(h->stream));
     const size_t row = 1 + 2 * (size_t)h->nz_max;
-    if (dalloc(h, &h->stats_part, (size_t)h->P.ntiles * h->nz_max * 2)) return DHARA_ERR_NOMEM;
+    if (dalloc(h, &h->stats_part, h->tiles_cap * h->nz_max * 2)) return DHARA_ERR_NOMEM;
     if (dalloc(h, &h->stats_hist, (size_t)h->ndom * max_steps * row)) return DHARA_ERR_NOMEM;
     CK(cudaMemsetAsync(h->stats_hist, 0, (size_t)h->ndom * max_steps * row * 8, h->stream));
     h->stats_steps = max_steps;
@@ -584,11 +645,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         D.overland_tol = p.overland_tol;
         D.closure_fp32 = (h->mixed && p.closure_fp32) ? 1 : 0;
         D.closure_fast = (h->mixed && !p.closure_fp32) ? 1 : 0;
-        D.record_branches = p.record_branches ? 1 : 0;
-        D.tile_begin = (int)h->htiles.size();
-        for (int y0 = 0; y0 < p.ny; y0 += TILE_Y)
-            for (int x0 = 0; x0 < p.nx; x0 += TILE_X) h->htiles.push_back({d, x0, y0, 0});
-        D.tile_end = (int)h->htiles.size();
+        D.record_branches = p.record_branches & 127;
         // overland segments: runs of up to OLF_SEG surface cells of this domain
         {
             const int first = (int)h->hsegs.size();
@@ -609,6 +666,10 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         if (p.nz > h->nz_max) h->nz_max = p.nz;
         if (p.picard_maxiter > h->maxiter_picard) h->maxiter_picard = p.picard_maxiter;
     }
+    // tile lists: room for either shape's list, the per-domain plan by default
+    for (int d = 0; d < ndomains; ++d)
+        h->tiles_cap += std::max(tile_count(h->hdom[d], TILE_X, TILE_Y), tile_count(h->hdom[d], 16, 8));
+    plan_tiles(h, 0);
     h->nproc.assign(ndomains, 1);
     h->roots.assign(ndomains, std::vector<double>());
     h->sched.assign(ndomains, std::vector<double>());
@@ -621,7 +682,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     int rc = 0;
     rc |= dalloc(h, &h->d_dom, ndomains);
     TileDesc *d_tiles = nullptr;
-    rc |= dalloc(h, &d_tiles, h->htiles.size());
+    rc |= dalloc(h, &d_tiles, h->tiles_cap);
     for (double **q : {&P.psin, &P.thetan, &P.psim, &P.x, &P.b, &P.ksat}) rc |= dalloc(h, q, N);
     for (void **q : {&P.K, &P.D, &P.p0, &P.p1, &P.z0, &P.z1, &P.t0, &P.t1, &P.d, &P.finv, &P.fc})
         rc |= dalloc_void(h, q, N * sT);
@@ -665,7 +726,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     rc |= dalloc(h, &P.diag, ndomains);
     rc |= dalloc(h, &P.gctrl, 1);
     rc |= dalloc(h, &P.barrier, 1);
-    rc |= dalloc(h, &P.partials, h->htiles.size() * NPART);
+    rc |= dalloc(h, &P.partials, h->tiles_cap * NPART);
     rc |= dalloc(h, &P.arrive, (size_t)ndomains * 4);
     rc |= dalloc(h, &P.step_acc, (size_t)ndomains * 16);
     if (rc) return bail(DHARA_ERR_NOMEM);
@@ -715,7 +776,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     e = e ? e : zero(P.diag, ndomains * sizeof(DevDiag));
     e = e ? e : zero(P.gctrl, sizeof(GlobalCtrl));
     e = e ? e : zero(P.barrier, sizeof(GridBarrier));
-    e = e ? e : zero(P.partials, h->htiles.size() * NPART * 8);
+    e = e ? e : zero(P.partials, h->tiles_cap * NPART * 8);
     e = e ? e : zero(P.arrive, (size_t)ndomains * 4 * 4);
     e = e ? e : zero(P.step_acc, (size_t)ndomains * 16 * 8);
     if (e != cudaSuccess) return bail(fail(DHARA_ERR_CUDA, "initialising device memory: %s", cudaGetErrorString(e)));
@@ -1037,6 +1098,7 @@ int dhara_step(dhara_handle *h, int nsteps, int use_graph) {
         int rc = enqueue_subsurface(h);
         if (!rc) rc = enqueue_overland(h);
         cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        h->graph_launches = h->launch_count - lc;  // the kernels one replay runs
         h->launch_count = lc;
         if (rc == DHARA_OK && e == cudaSuccess) e = cudaGraphInstantiate(&h->graph_exec, g, 0);
         if (g) cudaGraphDestroy(g);
@@ -1049,8 +1111,7 @@ int dhara_step(dhara_handle *h, int nsteps, int use_graph) {
     for (int s = 0; s < nsteps; ++s) {
         if (use_graph && h->graph_exec && !h->timing) {
             CK(cudaGraphLaunch(h->graph_exec, h->stream));
-            h->launch_count += 4 + 3 * (long long)h->maxiter_picard + 3 + (h->stats_steps > 0 ? 2 : 0) +
-                               (h->any_dirichlet ? 2 * (long long)h->maxiter_picard : 0);
+            h->launch_count += h->graph_launches;
         } else {
             int rc = enqueue_subsurface(h);
             if (rc) return rc;
@@ -1518,6 +1579,8 @@ void fill_config(const dhara_handle *h, dhara_launch_config *out) {
     out->krylov_blocks_per_sm = h->L.krylov_per_sm;
     out->overland_resident = h->L.olf_allow_resident;
     out->overland_blocks_per_sm = h->L.olf_stream_per_sm;
+    out->tile_shape = h->tile_mode;
+    out->fused_step = h->L.fused_step;
 }
 
 }  // namespace
@@ -1534,9 +1597,19 @@ int dhara_set_launch_config(dhara_handle *h, const dhara_launch_config *cfg) {
         cfg->overland_blocks_per_sm < 1 || cfg->overland_blocks_per_sm > h->L.olf_stream_per_sm_max)
         return fail(DHARA_ERR_INVALID, "blocks per SM must be in [1, %d] (Krylov) and [1, %d] (overland)",
                     h->L.krylov_per_sm_max, h->L.olf_stream_per_sm_max);
+    if (cfg->tile_shape < 0 || cfg->tile_shape > 2)
+        return fail(DHARA_ERR_INVALID, "tile_shape must be 0 (per domain), 1 (32 x 4) or 2 (16 x 8)");
+    if (cfg->fused_step && h->L.step_per_sm < cfg->krylov_blocks_per_sm)
+        return fail(DHARA_ERR_INVALID, "the fused step runs at most %d blocks per SM", h->L.step_per_sm);
     if (set_dev(h)) return DHARA_ERR_CUDA;
     CK(cudaStreamSynchronize(h->stream));
+    if (cfg->tile_shape != h->tile_mode) {
+        plan_tiles(h, cfg->tile_shape);
+        const int rc = apply_tiles(h);
+        if (rc) return rc;
+    }
     h->L.krylov_per_sm = cfg->krylov_blocks_per_sm;
+    h->L.fused_step = cfg->fused_step ? 1 : 0;
     h->L.olf_allow_resident = cfg->overland_resident ? 1 : 0;
     h->L.olf_stream_per_sm = cfg->overland_blocks_per_sm;
     if (h->graph_exec) {  // launch dimensions are baked into the graph
@@ -1563,11 +1636,18 @@ int dhara_autotune(dhara_handle *h, int trial_steps, dhara_launch_config *chosen
     std::memcpy(saved_n, h->launches, sizeof(saved_n));
     const long long saved_count = h->launch_count;
     h->timing = true;
+    // kind < 0: every kernel of the step
+    auto timed_ms = [&](int kind) {
+        if (kind >= 0) return h->total_ms[kind];
+        double s = 0.0;
+        for (int k = 0; k < KT_N; ++k) s += h->total_ms[k];
+        return s;
+    };
     auto trial = [&](int kind, double *ms) -> int {
         int r = restore_state(h, st);
         if (r) return r;
         collect_timing(h);
-        const double before = h->total_ms[kind];
+        const double before = timed_ms(kind);
         for (int t = 0; t < trial_steps && !r; ++t) {
             r = enqueue_subsurface(h);
             if (!r) r = enqueue_overland(h);
@@ -1577,10 +1657,35 @@ int dhara_autotune(dhara_handle *h, int trial_steps, dhara_launch_config *chosen
         r = check_device_error(h);
         if (r) return r;
         collect_timing(h);
-        *ms = (h->total_ms[kind] - before) / trial_steps;
+        *ms = (timed_ms(kind) - before) / trial_steps;
         return DHARA_OK;
     };
     LaunchCfg &L = h->L;
+    L.fused_step = 0;  // the stages below time kernels by name
+    // tile shape: the whole step's time (every 3D kernel works on the tiles);
+    // plans that come out the same for every domain are timed once
+    {
+        const int mode0 = h->tile_mode;
+        int best_mode = mode0;
+        double best_ms = 1e300;
+        std::vector<std::vector<int>> seen;
+        for (int mode = 0; mode <= 2 && !rc; ++mode) {
+            plan_tiles(h, mode);
+            std::vector<int> shape;
+            for (const DomainDesc &D : h->hdom) shape.push_back(D.tx);
+            bool dup = false;
+            for (const auto &s2 : seen) dup = dup || s2 == shape;
+            if (dup) continue;
+            seen.push_back(shape);
+            rc = apply_tiles(h);
+            double ms = 0;
+            if (!rc) rc = trial(-1, &ms);
+            if (!rc && ms < best_ms) { best_ms = ms; best_mode = mode; }
+        }
+        plan_tiles(h, rc ? mode0 : best_mode);
+        const int r2 = apply_tiles(h);
+        if (!rc) rc = r2;
+    }
     // 3D Krylov: blocks per SM
     int best_k = L.krylov_per_sm;
     double best_kms = 1e300;
@@ -1609,6 +1714,17 @@ int dhara_autotune(dhara_handle *h, int trial_steps, dhara_launch_config *chosen
     }
     L.olf_allow_resident = best_res;
     L.olf_stream_per_sm = best_ob;
+    // one launch per subsurface step, or one per kernel: the whole step's time
+    if (!rc && L.step_per_sm >= L.krylov_per_sm) {
+        double ms_sep = 0, ms_fused = 0;
+        L.fused_step = 0;
+        rc = trial(-1, &ms_sep);
+        if (!rc) {
+            L.fused_step = 1;
+            rc = trial(-1, &ms_fused);
+        }
+        L.fused_step = (!rc && ms_fused < ms_sep) ? 1 : 0;
+    }
     h->timing = timing_was;
     const int rr = restore_state(h, st);
     std::memcpy(h->total_ms, saved_ms, sizeof(saved_ms));

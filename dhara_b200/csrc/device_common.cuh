@@ -219,7 +219,14 @@ __device__ __forceinline__ bool domain_reduce(const DevPtrs &P, int tile, int do
 // took the same decisions everywhere have equal sums and any differing
 // decision changes the sum (barring a 2^-64 coincidence).  mix is the
 // splitmix64 finaliser (Steele, Lea & Flood 2014).
-enum { BR_TOPFLUX = 1, BR_PONDCLIP = 2, BR_MANNING = 3, BR_DEPTHCLIP = 4, BR_SATURATION = 5, BR_PICARD = 6 };
+enum { BR_TOPFLUX = 1, BR_PONDCLIP = 2, BR_MANNING = 3, BR_DEPTHCLIP = 4, BR_SATURATION = 5, BR_PICARD = 6,
+       BR_OLFITER = 7 };
+
+// whether decisions of `kind` are recorded (DomainDesc::record_branches is a
+// bit mask, bit kind - 1)
+__device__ __forceinline__ bool records(const DomainDesc &D, int kind) {
+    return (D.record_branches >> (kind - 1)) & 1;
+}
 
 __device__ __forceinline__ unsigned long long branch_mix(int step, int kind, long long index, unsigned code) {
     unsigned long long x = ((unsigned long long)(unsigned)step << 40) ^ ((unsigned long long)kind << 36) ^
@@ -380,6 +387,7 @@ __device__ __forceinline__ double vg_theta(double psi, double alpha_m, double n,
 // Column geometry of a thread inside its tile.
 struct ColumnRef {
     int dom, i, j, nx, ny, nz, nxp;
+    int tx, ty, tx_log2;  // the tile's shape
     long long g0, sxy;   // cell (i,j,0) index and plane stride
     long long c;         // column index in 2D arrays
     bool valid;
@@ -390,8 +398,11 @@ __device__ __forceinline__ ColumnRef column_of(const DevPtrs &P, int tile) {
     const DomainDesc &D = P.dom[t.dom];
     ColumnRef r;
     r.dom = t.dom;
-    r.i = t.x0 + (threadIdx.x % TILE_X);
-    r.j = t.y0 + (threadIdx.x / TILE_X);
+    r.tx = D.tx;
+    r.ty = D.ty;
+    r.tx_log2 = D.tx_log2;
+    r.i = t.x0 + ((int)threadIdx.x & (D.tx - 1));
+    r.j = t.y0 + ((int)threadIdx.x >> D.tx_log2);
     r.nx = D.nx;
     r.ny = D.ny;
     r.nz = D.nz;

@@ -14,6 +14,8 @@
 
 #include "../../include/dhara_gpu.h"
 
+// Default tile shape; a domain may use 16 x 8 instead (DomainDesc::tx, ty:
+// tx * ty = TILE_THREADS always, tx a power of two)
 #define TILE_X 32
 #define TILE_Y 4
 #define TILE_THREADS (TILE_X * TILE_Y)
@@ -37,13 +39,13 @@
 // whether the FP32 column solve keeps its forward-sweep values d' in shared
 // memory (1) or in the t array it then overwrites (0)
 #ifndef KRYLOV_BLOCKS_F32
-#define KRYLOV_BLOCKS_F32 5
+#define KRYLOV_BLOCKS_F32 7
 #endif
 #ifndef KRYLOV_BLOCKS_F64
 #define KRYLOV_BLOCKS_F64 4
 #endif
 #ifndef KRYLOV_DSMEM_F32
-#define KRYLOV_DSMEM_F32 1
+#define KRYLOV_DSMEM_F32 0
 #endif
 
 // Tensor maps of one domain (index = dom * NMAP + id): halo boxes
@@ -69,7 +71,7 @@ struct DomainDesc {
     int krylov_maxiter, inner_maxiter, overland_maxiter, sched_len;
     int tile_begin, tile_end, closure_fp32, nxp;  // nxp: row pitch of 3D arrays (nx rounded up to 4)
     int closure_fast, has_dirichlet;              // reformulated FP64 closure (mixed mode); any type-0 face
-    int record_branches, pad_rb;                  // accumulate DevDiag::branch_sig
+    int record_branches, tx, ty, tx_log2;         // accumulate DevDiag::branch_sig; tile shape
     long long off3, off2, offWE, offSN, sched_off;
     double dx, dy, dz, dt;
     double alpha, n, theta_s, theta_r, porosity, Ss, am;
@@ -90,14 +92,15 @@ struct KrylovCtrl {
     double rz;          // preconditioned residual norm r.M^-1 r after the last inner iteration
     double alpha, beta; // step of the last inner iteration (its x update is pending) and the next beta
     double inner_target2;  // the inner solve stops when rz falls to this
+    double rho_last;    // z.M z of the last inner iteration (the rho its direction p was formed with)
     int active;         // outer solve still running
     int inner_active;   // inner PCG running
     int inner_iter;     // inner iterations in the current cycle
     int total_iter;     // inner iterations this solve
     int cycles;         // outer residual recomputes this solve
     int parity;         // which z/t/p buffers hold the last iteration's vectors
-    int first_inner;
-    int pad;
+    int first_inner;    // next sweep is a cycle's first: z from phase R, no pending update
+    int keep_p;         // ... and it continues the previous cycle's direction p (beta != 0)
 };
 
 struct PicardCtrl {
@@ -163,6 +166,8 @@ struct GlobalCtrl {
     int n_olf_active;
     unsigned int olf_bar;  // arrivals at the resident overland solve's barrier
     int olf_live[4];     // domains still iterating, rotating over three phases
+    int n_picard;        // domains whose Picard iteration is not done this step (k_step)
+    int pad_g;
 };
 
 // Number of double partial sums per tile kept for reductions.
@@ -230,6 +235,9 @@ struct LaunchCfg {
     int smem_3d;          // dynamic shared memory bytes of the 3D solve
     int nz_max;
     int mixed;
+    int step_per_sm;      // co-resident blocks per SM of the fused step kernel
+    int fused_step;       // run the subsurface step as one launch (k_step)
+    int uniform_tx;       // the tile width shared by every domain (32 or 16), 0 if they differ
 };
 
 cudaError_t launch_psi_from_theta(const DevPtrs &P, cudaStream_t s);
@@ -237,6 +245,9 @@ cudaError_t launch_prepare(const DevPtrs &P, int mixed, cudaStream_t s);
 cudaError_t launch_prologue(const DevPtrs &P, cudaStream_t s);
 cudaError_t launch_assemble(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
 cudaError_t launch_krylov(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
+// prologue, Picard loop (assembly, Dirichlet passes, solve, check) and
+// epilogue of a subsurface step in one persistent launch
+cudaError_t launch_step(const DevPtrs &P, const LaunchCfg &L, int maxiter, int dirichlet, cudaStream_t s);
 cudaError_t launch_dirichlet(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
 cudaError_t launch_picard_check(const DevPtrs &P, cudaStream_t s);
 cudaError_t launch_epilogue(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);

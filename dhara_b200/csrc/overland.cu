@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_olf_setup(DevPtrs P, long long
             const double Sss = sqrt(pow((Hs_ - Hs_mN) / dy, 2.) +
                                     pow((Hs_p1 + Hs_mNp1 - Hs_m1 - Hs_mNm1) / (4 * dx), 2.));
             ks = manning_k(Hs_mN, h_mN, mann_mN, Hs_, h_, mann_, Sss, D, ws);
-            if (D.record_branches)
+            if (records(D, BR_MANNING))
                 bsig = branch_mix(P.pctrl[td.dom].step, BR_MANNING, I, ((we * 27u + ww) * 27u + wn) * 27u + ws);
         }
         P.olf_k[0 * ctot + I] = kw;
@@ -670,7 +670,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_olf_finish(DevPtrs P, long lon
         P.h[I] = hn;
         P.ph[I] = hn;
         if (d < 0) v[1] = -d;
-        if (D.record_branches) bsig = branch_mix(P.pctrl[td.dom].step, BR_DEPTHCLIP, I, band3(d, 0.0, 1e-9));
+        if (records(D, BR_DEPTHCLIP)) bsig = branch_mix(P.pctrl[td.dom].step, BR_DEPTHCLIP, I, band3(d, 0.0, 1e-9));
         v[2] = hn;
         if (!is_ring(cr.i, cr.j, cr.nx, cr.ny)) {
             const OlfRow w = olf_row(P, cr, D, ctot);
@@ -688,6 +688,8 @@ __global__ void __launch_bounds__(TILE_THREADS) k_olf_finish(DevPtrs P, long lon
         dg.olf_clip_cum += v[1];
         dg.ponded = v[2];
         dg.overland_iters_total += oc.iter;
+        if (records(D, BR_OLFITER))
+            atomicAdd(&dg.branch_sig, branch_mix(P.pctrl[td.dom].step, BR_OLFITER, td.dom, (unsigned)oc.iter));
         const double tol2 = D.overland_tol * D.overland_tol;
         if (!(oc.rr <= tol2 * oc.bb)) dg.overland_nonconverged += 1;
     }

@@ -1,18 +1,19 @@
 // staging.cuh -- TMA staging of a column tile's z-planes into shared memory.
 //
-// A block owns a tile of TILE_X x TILE_Y columns and marches down k.  Each
+// A block owns a tile of tx x ty columns and marches down k.  Each
 // input array of a sweep is copied chunk by chunk (CH planes at a time) into
 // shared memory by the Tensor Memory Accelerator: one thread arms the chunk's
 // mbarrier with the expected byte count and issues one
 // cp.async.bulk.tensor.3d per array; all threads wait on the mbarrier.  Two
 // buffers alternate, so chunk s+1 streams in while chunk s is consumed.
 //
-// Boxes (x, y, z), all starting at 16-byte aligned x (the TMA rule):
+// Boxes (x, y, z) for a tile of tx x ty columns, all starting at 16-byte
+// aligned x (the TMA rule):
 //   halo arrays (read at x/y neighbours): x from x0 - XOFF, width
-//     BW = TILE_X + 2*XOFF with XOFF = 16 / sizeof(element), y from y0 - 1,
-//     height TILE_Y + 2;  shared layout [CH][TILE_Y+2][BW]
-//   own arrays (read at the thread's column): x0, y0, TILE_X x TILE_Y;
-//     shared layout [CH][TILE_Y*TILE_X]
+//     BW = tx + 2*XOFF with XOFF = 16 / sizeof(element), y from y0 - 1,
+//     height ty + 2;  shared layout [CH][ty+2][BW]
+//   own arrays (read at the thread's column): x0, y0, tx x ty;
+//     shared layout [CH][ty*tx]
 // Coordinates outside the domain (including the negative halo origin) are
 // zero-filled by the TMA unit.  Loads only, never multicast.
 #pragma once
@@ -21,18 +22,21 @@
 
 #include "device_common.cuh"
 
-#define HY (TILE_Y + 2)
 #define OWN_PLANE TILE_THREADS
 
+// Halo layout of a tile of tx x ty columns (tx * ty = TILE_THREADS): planes of
+// (tx + 2 XOFF) x (ty + 2) elements.  The two supported shapes, 32 x 4 and
+// 16 x 8, have equal planes in FP32 (40 x 6 = 24 x 10 = 240) and nearly equal
+// ones in FP64 (36 x 6 = 216, 20 x 10 = 200), so one slot size serves both.
 template <typename V>
 struct Halo {
     static constexpr int XOFF = 16 / (int)sizeof(V);
-    static constexpr int BW = TILE_X + 2 * XOFF;
-    static constexpr int PLANE = HY * BW;
-    // shared index of the thread's own column in a halo plane
-    static __device__ __forceinline__ int center() {
-        return ((threadIdx.x / TILE_X) + 1) * BW + (threadIdx.x % TILE_X) + XOFF;
-    }
+    static constexpr int P32 = (32 + 2 * XOFF) * (4 + 2), P16 = (16 + 2 * XOFF) * (8 + 2);
+    static constexpr int PLANE_MAX = P32 > P16 ? P32 : P16;
+    int bw, plane, hc;  // row width, plane size, the thread's own column
+    __device__ __forceinline__ Halo(int tx, int tx_log2, int ty)
+        : bw(tx + 2 * XOFF), plane((tx + 2 * XOFF) * (ty + 2)),
+          hc((((int)threadIdx.x >> tx_log2) + 1) * (tx + 2 * XOFF) + ((int)threadIdx.x & (tx - 1)) + XOFF) {}
 };
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
@@ -99,20 +103,21 @@ __device__ __forceinline__ void tma_own(V *dst, const CUtensorMap *map, int x0, 
                                         uint64_t *bar) {
     tma_load_3d(dst, map, x0, y0, k0, bar);
 }
+// bytes of a halo box of CHN planes for a tile tx wide and ty high
 template <typename V, int CHN>
-constexpr unsigned halo_bytes() {
-    return (unsigned)(CHN * Halo<V>::PLANE * sizeof(V));
+__device__ __forceinline__ unsigned halo_bytes(int tx, int ty) {
+    return (unsigned)(CHN * (tx + 2 * Halo<V>::XOFF) * (ty + 2) * sizeof(V));
 }
 template <typename V, int CHN>
 constexpr unsigned own_bytes() {
     return (unsigned)(CHN * OWN_PLANE * sizeof(V));
 }
-// Stride of a halo box's slot in a staging buffer: the TMA writes shared
-// memory at 128-byte aligned addresses, so each slot is the box's bytes
-// rounded up to 128 (the transaction count stays halo_bytes).
+// Stride of a halo box's slot in a staging buffer: the largest box of the
+// supported shapes, rounded up to 128 bytes (the TMA writes shared memory at
+// 128-byte aligned addresses); the transaction count stays halo_bytes.
 template <typename V, int CHN>
 constexpr unsigned halo_slot() {
-    return (halo_bytes<V, CHN>() + 127u) & ~127u;
+    return ((unsigned)(CHN * Halo<V>::PLANE_MAX * sizeof(V)) + 127u) & ~127u;
 }
 
 // Block-uniform state of the staging buffers: mbarriers and the parity each

@@ -87,8 +87,7 @@ __global__ void k_prepare(DevPtrs P) {
 // IdentifyTopBoundary (206-257).  The top flux does not change between Picard
 // iterations (its inputs hpoten, qcapa, theta^n, Ks are fixed for the step), so
 // it is evaluated once per step.  Also resets the per-step control state.
-__global__ void k_prologue(DevPtrs P) {
-    const int tile = blockIdx.x;
+__device__ __forceinline__ void prologue_tile(const DevPtrs &P, int tile) {
     const ColumnRef cr = column_of(P, tile);
     const DomainDesc &D = P.dom[cr.dom];
     const TileDesc td = P.tiles[tile];
@@ -97,6 +96,7 @@ __global__ void k_prologue(DevPtrs P) {
             P.gctrl->n_active = 0;
             P.gctrl->n_inner_active = 0;
             P.gctrl->n_olf_active = 0;
+            P.gctrl->n_picard = P.ndom;
         }
         if (tile == D.tile_begin) {
             PicardCtrl &pc = P.pctrl[td.dom];
@@ -141,9 +141,13 @@ __global__ void k_prologue(DevPtrs P) {
         }
         P.hpoten[c] = hpoten;
         P.qtop[c] = q;
-        if (D.record_branches) bsig = branch_mix(step, BR_TOPFLUX, c, code);
+        if (records(D, BR_TOPFLUX)) bsig = branch_mix(step, BR_TOPFLUX, c, code);
     }
     if (D.record_branches) branch_commit(&P.diag[td.dom].branch_sig, bsig);
+}
+
+__global__ void k_prologue(DevPtrs P) {
+    prologue_tile(P, blockIdx.x);
 }
 
 // -------------------------------------------------------------- assembly
@@ -159,8 +163,7 @@ __global__ void k_prologue(DevPtrs P) {
 // Eight blocks per SM (64 registers): the FP64 closure's latency chains need the
 // warps more than the registers (measured 18 % faster than the uncapped 96).
 template <typename T>
-__global__ void __launch_bounds__(TILE_THREADS, 8) k_assemble(DevPtrs P) {
-    const int tile = blockIdx.x;
+__device__ __forceinline__ void assemble_tile(const DevPtrs &P, int tile) {
     const TileDesc td = P.tiles[tile];
     const DomainDesc &D = P.dom[td.dom];
     const PicardCtrl &pc = P.pctrl[td.dom];
@@ -174,11 +177,13 @@ __global__ void __launch_bounds__(TILE_THREADS, 8) k_assemble(DevPtrs P) {
         kc.total_iter = 0;
         kc.parity = 0;
         kc.first_inner = 1;
+        kc.keep_p = 0;
+        kc.rho_last = 0.0;
         if (!done) atomicAdd(&P.gctrl->n_active, 1);
     }
     if (done) return;
     const ColumnRef cr = column_of(P, tile);
-    if (D.record_branches) {
+    if (records(D, BR_SATURATION)) {
         // saturation (psi >= 0 switches the closure's branch) of every cell at psi^m
         unsigned long long bsig = 0;
         if (cr.valid) {
@@ -259,6 +264,11 @@ __global__ void __launch_bounds__(TILE_THREADS, 8) k_assemble(DevPtrs P) {
         K_c = K_n;
         C_c = C_n;
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TILE_THREADS, 8) k_assemble(DevPtrs P) {
+    assemble_tile<T>(P, blockIdx.x);
 }
 
 // ---------------------------------------------------------- Dirichlet faces
@@ -345,8 +355,7 @@ __device__ __forceinline__ bool dir_rules(const ColumnRef &cr, int k, const DirF
 
 // Pass 1: identity rows (D = -1, x = b = the row's right-hand side).
 template <typename T>
-__global__ void __launch_bounds__(TILE_THREADS) k_dir_fixed(DevPtrs P) {
-    const int tile = blockIdx.x;
+__device__ __forceinline__ void dir_fixed_tile(const DevPtrs &P, int tile) {
     const TileDesc td = P.tiles[tile];
     const DomainDesc &D = P.dom[td.dom];
     if (!D.has_dirichlet || P.pctrl[td.dom].done) return;
@@ -365,11 +374,15 @@ __global__ void __launch_bounds__(TILE_THREADS) k_dir_fixed(DevPtrs P) {
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(TILE_THREADS) k_dir_fixed(DevPtrs P) {
+    dir_fixed_tile<T>(P, blockIdx.x);
+}
+
 // Pass 2: the rows next to identity rows get the reference's elimination
 // terms, less the coupling the matrix-free stencil applies to the fixed value.
 template <typename T>
-__global__ void __launch_bounds__(TILE_THREADS) k_dir_rows(DevPtrs P) {
-    const int tile = blockIdx.x;
+__device__ __forceinline__ void dir_rows_tile(const DevPtrs &P, int tile) {
     const TileDesc td = P.tiles[tile];
     const DomainDesc &D = P.dom[td.dom];
     if (!D.has_dirichlet || P.pctrl[td.dom].done) return;
@@ -391,6 +404,11 @@ __global__ void __launch_bounds__(TILE_THREADS) k_dir_rows(DevPtrs P) {
         if (f.e && cr.i == cr.nx - 2) v -= ix2 * fk.ke * P.x[g + 1];
         P.b[g] = v;
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TILE_THREADS) k_dir_rows(DevPtrs P) {
+    dir_rows_tile<T>(P, blockIdx.x);
 }
 
 // ------------------------------------------------------------ Krylov solve
@@ -559,10 +577,12 @@ template <typename T>
 __device__ __forceinline__ void issue_R(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
                                         StageBars &sb) {
     constexpr int CHN = CH_R;
-    constexpr unsigned HB = halo_bytes<double, CHN>(), HS = halo_slot<double, CHN>();
+    constexpr unsigned HS = halo_slot<double, CHN>();
     constexpr unsigned OB = own_bytes<double, CHN>();
     static_assert(HS % 128 == 0 && OB % 128 == 0, "TMA destinations must be 128-byte aligned");
     const TileDesc td = P.tiles[tile];
+    const DomainDesc &D = P.dom[td.dom];
+    const unsigned HB = halo_bytes<double, CHN>(D.tx, D.ty);
     const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
     unsigned char *B = stage + b * StageSize<T>::buffer();
     const int k0 = st * CHN;
@@ -576,24 +596,26 @@ __device__ __forceinline__ void issue_R(const DevPtrs &P, int tile, int st, int 
 
 // The inner sweep's chunk: the previous iteration's z, t, p (buffers `prev`)
 // and K at the halo, D, 1/den, c' and d at the own columns.  The first sweep of
-// a cycle has no previous t, p or d (alpha = beta = 0, d starts at zero).
+// a cycle has no previous t or d (alpha = 0, d starts at zero), and no p
+// either unless it continues the previous cycle's direction (keep_p).
 template <typename T>
 __device__ __forceinline__ void issue_C(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
-                                        StageBars &sb, bool first, int prev) {
+                                        StageBars &sb, bool first, bool keep_p, int prev) {
     constexpr int CHN = Chunk<T>::inner;
-    constexpr unsigned HB = halo_bytes<T, CHN>(), HS = halo_slot<T, CHN>(), OB = own_bytes<T, CHN>();
+    constexpr unsigned HS = halo_slot<T, CHN>(), OB = own_bytes<T, CHN>();
     static_assert(HS % 128 == 0 && OB % 128 == 0, "TMA destinations must be 128-byte aligned");
     const TileDesc td = P.tiles[tile];
+    const DomainDesc &D = P.dom[td.dom];
+    const unsigned HB = halo_bytes<T, CHN>(D.tx, D.ty);
     const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
     unsigned char *B = stage + b * StageSize<T>::buffer();
     const int k0 = st * CHN;
+    const bool with_p = !first || keep_p;
     sb.issued(b);
-    mbar_expect_tx(sb.bar + b, (first ? 2 : 4) * HB + (first ? 3 : 4) * OB);
+    mbar_expect_tx(sb.bar + b, (first ? 2 : 3) * HB + (with_p ? HB : 0) + (first ? 3 : 4) * OB);
     tma_halo<T, CHN>((T *)B, maps + (prev ? MAP_Z1_H : MAP_Z0_H), td.x0, td.y0, k0, sb.bar + b);
-    if (!first) {
-        tma_halo<T, CHN>((T *)(B + HS), maps + (prev ? MAP_T1_H : MAP_T0_H), td.x0, td.y0, k0, sb.bar + b);
-        tma_halo<T, CHN>((T *)(B + 2 * HS), maps + (prev ? MAP_P1_H : MAP_P0_H), td.x0, td.y0, k0, sb.bar + b);
-    }
+    if (!first) tma_halo<T, CHN>((T *)(B + HS), maps + (prev ? MAP_T1_H : MAP_T0_H), td.x0, td.y0, k0, sb.bar + b);
+    if (with_p) tma_halo<T, CHN>((T *)(B + 2 * HS), maps + (prev ? MAP_P1_H : MAP_P0_H), td.x0, td.y0, k0, sb.bar + b);
     tma_halo<T, CHN>((T *)(B + 3 * HS), maps + MAP_K_H, td.x0, td.y0, k0, sb.bar + b);
     tma_own<T, CHN>((T *)(B + 4 * HS), maps + MAP_D_O, td.x0, td.y0, k0, sb.bar + b);
     tma_own<T, CHN>((T *)(B + 4 * HS + OB), maps + MAP_INV_O, td.x0, td.y0, k0, sb.bar + b);
@@ -610,16 +632,20 @@ __device__ __forceinline__ void issue_head(int nz, Issue issue) {
 // ---- phase R: outer FP64 residual and the preconditioner factors -------------
 // r = b - A x with the FP64 coefficients, r_T = (T) r; the column factors of M
 // (1/den and c') from the inner operator's T coefficients (the same rounding as
-// the stored K, D) are stored; z = M^-1 r_T into z0 (the inner iteration's
-// "previous" z, buffer 0); v = {||r||^2, ||b||^2, r.z}.
+// the stored K, D) are stored; z = M^-1 r_T into the z buffer of the domain's
+// current parity (where the next sweep reads it, beside the last p);
+// v = {||r||^2, ||b||^2, r.z}.
 // Staged: x, K64 (halo), D64, b (own).
-template <typename T, bool DSMEM>
-__device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetched, const ColumnRef &cr,
+template <typename T, bool DSMEM, int TXC>
+__device__ __forceinline__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetched, const ColumnRef &cr,
                         const StencilW<T> &w, T *s_d, unsigned char *stage, StageBars &sb, double (&v)[3]) {
     constexpr int CHN = CH_R;
-    typedef Halo<double> H;
+    // the tile shape is a compile-time constant of each instantiation
+    const Halo<double> H(TXC, TXC == 32 ? 5 : 4, TILE_THREADS / TXC);
     constexpr unsigned HB = halo_slot<double, CHN>(), OB = own_bytes<double, CHN>();
-    T *__restrict__ z = (T *)P.z0;
+    // z goes into the buffer that holds the last iteration's p (the next
+    // sweep reads both from there)
+    T *__restrict__ z = (T *)(ldcg(&P.kctrl[P.tiles[tile].dom].parity) ? P.z1 : P.z0);
     T *__restrict__ finv = (T *)P.finv;
     T *__restrict__ fc = (T *)P.fc;
     const size_t BUF = StageSize<T>::buffer();
@@ -630,25 +656,25 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
             issue_head<CHN>(P.dom[P.tiles[tile_next].dom].nz,
                             [&](int st, int b) { issue_R<T>(P, tile_next, st, b, stage, sb); });
     };
-    const int nz = cr.nz, hc = H::center(), oc = threadIdx.x;
+    const int nz = cr.nz, hc = H.hc, oc = threadIdx.x;
     const Masks M = masks_of(cr);
     const double cx = (double)w.cx, cy = (double)w.cy, cz = (double)w.cz;
     double x_up = 0.0, K_up = 0.0;
     T cprev = T(0), yprev = T(0);
     auto plane = [&](int b, int pl, int k) {
         if (!cr.valid) return;
-        const double *sx = (const double *)buf(b) + pl * H::PLANE;
-        const double *sK = (const double *)(buf(b) + HB) + pl * H::PLANE;
+        const double *sx = (const double *)buf(b) + pl * H.plane;
+        const double *sK = (const double *)(buf(b) + HB) + pl * H.plane;
         const double *sD = (const double *)(buf(b) + 2 * HB) + pl * OWN_PLANE;
         const double *sb_ = (const double *)(buf(b) + 2 * HB + OB) + pl * OWN_PLANE;
         const double xc = sx[hc], Kc = sK[hc];
         double x_dn = 0.0, K_dn = 0.0;
         if (k + 1 < nz) {
-            if (pl + 1 < CHN) { x_dn = sx[H::PLANE + hc]; K_dn = sK[H::PLANE + hc]; }
+            if (pl + 1 < CHN) { x_dn = sx[H.plane + hc]; K_dn = sK[H.plane + hc]; }
             else { x_dn = ((const double *)buf((b + 1) % STAGES))[hc]; K_dn = ((const double *)(buf((b + 1) % STAGES) + HB))[hc]; }
         }
         const double mu = k > 0 ? 1.0 : 0.0, md = k < nz - 1 ? 1.0 : 0.0;
-        const double Kw = sK[hc - 1], Ke = sK[hc + 1], Ks = sK[hc - H::BW], Kn = sK[hc + H::BW];
+        const double Kw = sK[hc - 1], Ke = sK[hc + 1], Ks = sK[hc - H.bw], Kn = sK[hc + H.bw];
         const double kd = mu * 0.5 * (Kc + K_up), ku = md * 0.5 * (Kc + K_dn);
         const double kw = M.w * 0.5 * (Kc + Kw), ke = M.e * 0.5 * (Kc + Ke);
         const double ks = M.s * 0.5 * (Kc + Ks), kn = M.n * 0.5 * (Kc + Kn);
@@ -657,7 +683,7 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
         // value, so its residual is zero and the preconditioner leaves it alone
         const bool fixed = Dk < 0.0;
         const double Ax = Dk * xc + cx * (kw * (xc - sx[hc - 1]) + ke * (xc - sx[hc + 1])) +
-                          cy * (ks * (xc - sx[hc - H::BW]) + kn * (xc - sx[hc + H::BW])) +
+                          cy * (ks * (xc - sx[hc - H.bw]) + kn * (xc - sx[hc + H.bw])) +
                           cz * (kd * (xc - x_up) + ku * (xc - x_dn));
         const double rk = fixed ? 0.0 : bk - Ax;
         v[0] += rk * rk;
@@ -689,18 +715,21 @@ __device__ void phase_R(const DevPtrs &P, int tile, int tile_next, bool prefetch
 }
 
 // ---- inner sweep C: one PCG iteration --------------------------------------
-// With ap = alpha_{i-1} and bt = beta_i (both zero in a cycle's first sweep):
+// With ap = alpha_{i-1} and bt = beta_i (ap zero in a cycle's first sweep, bt
+// too unless the sweep continues the previous cycle's direction):
 // z = z_prev - ap t_prev and p = z + bt p_prev at the own column and its four
 // lateral neighbours (from the staged halo boxes) and at k+1; q = A p;
 // t = M^-1 q by the stored factors (forward sweep in the march, back sweep
 // after it); d += ap p_prev.  Writes z, p, t into the buffers other than
 // `prev`, and v = {p.q, z.q, q.t, z.M z}.
-template <typename T, bool DSMEM>
-__device__ void phase_C(const DevPtrs &P, int tile, int tile_next, bool prefetched, bool first_next,
-                        int prev_next, const ColumnRef &cr, const StencilW<T> &w, T ap, T bt, bool first,
-                        int prev, T *s_d, unsigned char *stage, StageBars &sb, double (&v)[4]) {
+template <typename T, bool DSMEM, int TXC>
+__device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_next, bool prefetched, bool first_next,
+                        bool keep_next, int prev_next, const ColumnRef &cr, const StencilW<T> &w, T ap, T bt,
+                        bool first, bool keep_p, int prev, T *s_d, unsigned char *stage, StageBars &sb,
+                        double (&v)[4]) {
     constexpr int CHN = Chunk<T>::inner;
-    typedef Halo<T> H;
+    // the tile shape is a compile-time constant of each instantiation
+    const Halo<T> H(TXC, TXC == 32 ? 5 : 4, TILE_THREADS / TXC);
     constexpr unsigned HB = halo_slot<T, CHN>();
     constexpr int S = CHN * OWN_PLANE;
     T *__restrict__ z_out = (T *)(prev ? P.z0 : P.z1);
@@ -710,37 +739,37 @@ __device__ void phase_C(const DevPtrs &P, int tile, int tile_next, bool prefetch
     const T *__restrict__ fc = (const T *)P.fc;
     const size_t BUF = StageSize<T>::buffer();
     auto buf = [&](int b) { return stage + b * BUF; };
-    auto issue = [&](int st, int b) { issue_C<T>(P, tile, st, b, stage, sb, first, prev); };
+    auto issue = [&](int st, int b) { issue_C<T>(P, tile, st, b, stage, sb, first, keep_p, prev); };
     auto issue_next = [&]() {
         if (tile_next < P.ntiles)
             issue_head<CHN>(P.dom[P.tiles[tile_next].dom].nz, [&](int st, int b) {
-                issue_C<T>(P, tile_next, st, b, stage, sb, first_next, prev_next);
+                issue_C<T>(P, tile_next, st, b, stage, sb, first_next, keep_next, prev_next);
             });
     };
-    const int nz = cr.nz, hc = H::center(), oc = threadIdx.x;
+    const int nz = cr.nz, hc = H.hc, oc = threadIdx.x;
     const Masks M = masks_of(cr);
     const T mW = (T)M.w, mE = (T)M.e, mS = (T)M.s, mN = (T)M.n;
     T p_up = T(0), z_up = T(0), K_up = T(0), cprev = T(0), yprev = T(0);
     // this iteration's z and p at offset o of staged halo planes (z, t, p)
     auto zv = [&](const T *zz, const T *tt, int o) { return first ? zz[o] : zz[o] - ap * tt[o]; };
     auto pv = [&](const T *zz, const T *tt, const T *pp, int o) {
-        return first ? zz[o] : (zz[o] - ap * tt[o]) + bt * pp[o];
+        return first ? (keep_p ? zz[o] + bt * pp[o] : zz[o]) : (zz[o] - ap * tt[o]) + bt * pp[o];
     };
     auto plane = [&](int b, int pl, int k) {
         if (!cr.valid) return;
-        const T *sz = (const T *)buf(b) + pl * H::PLANE;
-        const T *st = (const T *)(buf(b) + HB) + pl * H::PLANE;
-        const T *sp = (const T *)(buf(b) + 2 * HB) + pl * H::PLANE;
-        const T *sK = (const T *)(buf(b) + 3 * HB) + pl * H::PLANE;
+        const T *sz = (const T *)buf(b) + pl * H.plane;
+        const T *st = (const T *)(buf(b) + HB) + pl * H.plane;
+        const T *sp = (const T *)(buf(b) + 2 * HB) + pl * H.plane;
+        const T *sK = (const T *)(buf(b) + 3 * HB) + pl * H.plane;
         const T *own = (const T *)(buf(b) + 4 * HB) + pl * OWN_PLANE + oc;
         const T Dk = own[0], inv = own[S], cp = own[2 * S];
         const T zc = zv(sz, st, hc), pc = pv(sz, st, sp, hc);
         T z_dn = T(0), p_dn = T(0), K_dn = T(0);
         if (k + 1 < nz) {
             if (pl + 1 < CHN) {
-                z_dn = zv(sz + H::PLANE, st + H::PLANE, hc);
-                p_dn = pv(sz + H::PLANE, st + H::PLANE, sp + H::PLANE, hc);
-                K_dn = sK[H::PLANE + hc];
+                z_dn = zv(sz + H.plane, st + H.plane, hc);
+                p_dn = pv(sz + H.plane, st + H.plane, sp + H.plane, hc);
+                K_dn = sK[H.plane + hc];
             } else {
                 const unsigned char *nb = buf((b + 1) % STAGES);
                 const T *nzz = (const T *)nb, *ntt = (const T *)(nb + HB), *npp = (const T *)(nb + 2 * HB);
@@ -753,10 +782,10 @@ __device__ void phase_C(const DevPtrs &P, int tile, int tile_next, bool prefetch
         const T mu = k > 0 ? T(1) : T(0), md = k < nz - 1 ? T(1) : T(0);
         const T kd = mu * (T(0.5) * (Kc + K_up)), ku = md * (T(0.5) * (Kc + K_dn));
         const T kw = mW * (T(0.5) * (Kc + sK[hc - 1])), ke = mE * (T(0.5) * (Kc + sK[hc + 1]));
-        const T ks = mS * (T(0.5) * (Kc + sK[hc - H::BW])), kn = mN * (T(0.5) * (Kc + sK[hc + H::BW]));
+        const T ks = mS * (T(0.5) * (Kc + sK[hc - H.bw])), kn = mN * (T(0.5) * (Kc + sK[hc + H.bw]));
         const bool fixed = Dk < T(0);  // Dirichlet cell: identity row, z = p = 0 there
         T q = Dk * pc + w.cx * (kw * (pc - pv(sz, st, sp, hc - 1)) + ke * (pc - pv(sz, st, sp, hc + 1))) +
-              w.cy * (ks * (pc - pv(sz, st, sp, hc - H::BW)) + kn * (pc - pv(sz, st, sp, hc + H::BW))) +
+              w.cy * (ks * (pc - pv(sz, st, sp, hc - H.bw)) + kn * (pc - pv(sz, st, sp, hc + H.bw))) +
               w.cz * (kd * (pc - p_up) + ku * (pc - p_dn));
         // (M z)_k with M the column's tridiagonal part of A
         T Mz = (Dk + w.cx * (kw + ke) + w.cy * (ks + kn)) * zc + w.cz * (kd * (zc - z_up) + ku * (zc - z_dn));
@@ -807,10 +836,14 @@ __device__ __forceinline__ void finalize_R(const DevPtrs &P, int dom, const doub
         atomicAdd(&P.gctrl->n_inner_active, 1);
         c.inner_iter = 0;
         c.first_inner = 1;
-        c.parity = 0;  // phase R left z in buffer 0
         c.rz = v[2];
         c.alpha = 0.0;
-        c.beta = 0.0;
+        // A later cycle continues the direction of the previous one: the true
+        // residual replaces the recursive one (z = M^-1 r from phase R) and
+        // p = z + beta p with beta = rho_true / rho_last ("reliable update"),
+        // so refinement does not discard the Krylov space built so far.
+        c.keep_p = (c.total_iter > 0 && c.rho_last > 0.0) ? 1 : 0;
+        c.beta = c.keep_p ? v[2] / c.rho_last : 0.0;
         // the inner solve reduces r.M^-1 r by inner_tol^2 (mixed mode), or far
         // enough that ||r|| should meet the outer tolerance (half of it, with
         // the M^-1-norm standing in for the 2-norm); R checks the true residual
@@ -823,27 +856,41 @@ __device__ __forceinline__ void stop_inner(const DevPtrs &P, KrylovCtrl &c) {
     atomicSub(&P.gctrl->n_inner_active, 1);
 }
 
+// Shared memory of the persistent 3D solve: [d' of the column solves (float
+// only)][STAGES staging buffers], the staging buffers 128-byte aligned for the
+// TMA, and the stage mbarriers (initialised here, once per launch).
 template <typename T>
-__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F32 : KRYLOV_BLOCKS_F64)
-    k_krylov(DevPtrs P) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t s_bar[STAGES];
-    constexpr bool DSMEM = sizeof(T) == 4 && KRYLOV_DSMEM_F32;
-    // dynamic shared memory: [d' of the column solves (float only)][STAGES
-    // staging buffers], the staging buffers 128-byte aligned for the TMA
+struct SolveSmem {
+    T *s_d;
+    unsigned char *stage;
+};
+
+template <typename T, bool DSMEM>
+__device__ __forceinline__ SolveSmem<T> solve_smem(const DevPtrs &P, unsigned char *smem_raw, uint64_t *s_bar) {
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-    T *s_d = reinterpret_cast<T *>(base);
     const size_t dprime_bytes = DSMEM ? (size_t)P.smem_nz * TILE_THREADS * sizeof(T) : 0;
-    unsigned char *stage_raw = base + ((dprime_bytes + 127) & ~(size_t)127);
     if (threadIdx.x == 0) {
         for (int q = 0; q < STAGES; ++q) mbar_init(&s_bar[q], 1);
         mbar_fence_init();
     }
     __syncthreads();
-    StageBars sb{s_bar, 0u, P.barrier, 0u};
+    return SolveSmem<T>{reinterpret_cast<T *>(base), base + ((dprime_bytes + 127) & ~(size_t)127)};
+}
+
+// The whole linear solve of one Picard iteration for every active domain (the
+// body of k_krylov, also run by k_step).  Returns false when a grid barrier
+// gave up (the handle's error flag is set); the block must then return.
+// TXC: the tile width when every domain of the handle has the same tile shape
+// (the sweeps are then compiled for it), 0 when shapes differ by domain (each
+// tile is dispatched to the sweep of its shape).
+template <typename T, bool DSMEM, int TXC>
+__device__ __forceinline__ bool krylov_solve(const DevPtrs &P, const SolveSmem<T> &sm, StageBars &sb) {
+    T *s_d = sm.s_d;
+    unsigned char *stage_raw = sm.stage;
     // every error exit first lets this block's in-flight stage copies land
     auto fail = [&]() {
         if (threadIdx.x == 0) sb.drain();
+        return false;
     };
     // next tile of this block with an active domain (stride gridDim.x)
     auto next_outer = [&](int t) {
@@ -867,7 +914,12 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F
                 const int dom = P.tiles[t].dom;
                 const ColumnRef cr = column_of(P, t);
                 double v[3] = {0.0, 0.0, 0.0};
-                phase_R<T, DSMEM>(P, t, tn, pre, cr, weights(dom), s_d, stage_raw, sb, v);
+                if constexpr (TXC != 0)
+                    phase_R<T, DSMEM, TXC>(P, t, tn, pre, cr, weights(dom), s_d, stage_raw, sb, v);
+                else if (cr.tx == TILE_X)
+                    phase_R<T, DSMEM, TILE_X>(P, t, tn, pre, cr, weights(dom), s_d, stage_raw, sb, v);
+                else
+                    phase_R<T, DSMEM, 16>(P, t, tn, pre, cr, weights(dom), s_d, stage_raw, sb, v);
                 pre = tn < P.ntiles;
                 if (domain_reduce<3>(P, t, dom, 0, v) && threadIdx.x == 0) finalize_R(P, dom, v);
                 t = tn;
@@ -882,7 +934,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F
         // a block reads it once per domain rather than once per tile.
         struct Ctl {
             int dom, active, parity;
-            bool first;
+            bool first, keep_p;
             double alpha, beta;
         };
         auto ctl_load = [&](Ctl &c, int dom) {
@@ -892,6 +944,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F
             c.active = ldcg(&k->inner_active);
             c.parity = ldcg(&k->parity);
             c.first = ldcg(&k->first_inner) != 0;
+            c.keep_p = ldcg(&k->keep_p) != 0;
             c.alpha = ldcg(&k->alpha);
             c.beta = ldcg(&k->beta);
         };
@@ -906,7 +959,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F
         };
         while (ldcg(&P.gctrl->n_inner_active) > 0) {
             bool pre = false;
-            Ctl cc{-1, 0, 0, false, 0.0, 0.0}, cn{-1, 0, 0, false, 0.0, 0.0};
+            Ctl cc{-1, 0, 0, false, false, 0.0, 0.0}, cn{-1, 0, 0, false, false, 0.0, 0.0};
             for (int t = next_live(cc, blockIdx.x); t < P.ntiles;) {
                 const int tn = next_live(cn, t + gridDim.x);
                 const int dom = P.tiles[t].dom;
@@ -914,10 +967,19 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F
                 const ColumnRef cr = column_of(P, t);
                 const DomainDesc &D = P.dom[dom];
                 const bool first_n = tn < P.ntiles ? cn.first : false;
+                const bool keep_n = tn < P.ntiles ? cn.keep_p : false;
                 const int prev_n = tn < P.ntiles ? cn.parity : 0;
                 double v[4] = {0.0, 0.0, 0.0, 0.0};
-                phase_C<T, DSMEM>(P, t, tn, pre, first_n, prev_n, cr, weights(dom), (T)cc.alpha, (T)cc.beta,
-                                  cc.first, cc.parity, s_d, stage_raw, sb, v);
+                if constexpr (TXC != 0)
+                    phase_C<T, DSMEM, TXC>(P, t, tn, pre, first_n, keep_n, prev_n, cr, weights(dom), (T)cc.alpha,
+                                           (T)cc.beta, cc.first, cc.keep_p, cc.parity, s_d, stage_raw, sb, v);
+                else if (cr.tx == TILE_X)
+                    phase_C<T, DSMEM, TILE_X>(P, t, tn, pre, first_n, keep_n, prev_n, cr, weights(dom),
+                                              (T)cc.alpha, (T)cc.beta, cc.first, cc.keep_p, cc.parity, s_d,
+                                              stage_raw, sb, v);
+                else
+                    phase_C<T, DSMEM, 16>(P, t, tn, pre, first_n, keep_n, prev_n, cr, weights(dom), (T)cc.alpha,
+                                          (T)cc.beta, cc.first, cc.keep_p, cc.parity, s_d, stage_raw, sb, v);
                 pre = tn < P.ntiles;
                 if (domain_reduce<4>(P, t, dom, 0, v) && threadIdx.x == 0) {
                     KrylovCtrl &c = P.kctrl[dom];
@@ -928,6 +990,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F
                     c.alpha = bad ? 0.0 : alpha;  // a broken iteration leaves x alone
                     c.beta = bad ? 0.0 : rho_next / rho;
                     c.rz = rho_next;
+                    c.rho_last = bad ? 0.0 : rho;
                     c.parity ^= 1;
                     c.first_inner = 0;
                     c.inner_iter += 1;
@@ -959,13 +1022,25 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F
         }
         if (!grid_sync(P.barrier)) return fail();
     }
+    return true;
 }
+
+template <typename T, int TXC>
+__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F32 : KRYLOV_BLOCKS_F64)
+    k_krylov(DevPtrs P) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar[STAGES];
+    constexpr bool DSMEM = sizeof(T) == 4 && KRYLOV_DSMEM_F32;
+    const SolveSmem<T> sm = solve_smem<T, DSMEM>(P, smem_raw, s_bar);
+    StageBars sb{s_bar, 0u, P.barrier, 0u};
+    krylov_solve<T, DSMEM, TXC>(P, sm, sb);
+}
+
 
 // ---------------------------------------------------------- Picard check
 // Max of |(psi^{m+1}-psi^m)/psi^{m+1}| (or the theta / absolute variants) per
 // domain, then the convergence decision and iteration bookkeeping.
-__global__ void __launch_bounds__(TILE_THREADS) k_picard_check(DevPtrs P) {
-    const int tile = blockIdx.x;
+__device__ __forceinline__ void picard_check_tile(const DevPtrs &P, int tile) {
     const TileDesc td = P.tiles[tile];
     if (tile == 0 && threadIdx.x == 0) {
         P.gctrl->n_active = 0;
@@ -1007,11 +1082,16 @@ __global__ void __launch_bounds__(TILE_THREADS) k_picard_check(DevPtrs P) {
         c.iter += 1;
         c.converged = v[0] < D.picard_tol;
         c.done = c.converged || c.iter >= D.picard_maxiter;
+        if (c.done) atomicSub(&P.gctrl->n_picard, 1);  // k_step's loop ends at zero
         dg.krylov_iters_total += kc.total_iter;
         dg.refine_iters_total += kc.cycles;
         dg.krylov_iters_last += kc.total_iter;
         dg.picard_err_last = v[0];
     }
+}
+
+__global__ void __launch_bounds__(TILE_THREADS) k_picard_check(DevPtrs P) {
+    picard_check_tile(P, blockIdx.x);
 }
 
 // -------------------------------------------------------------- epilogue
@@ -1024,8 +1104,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_picard_check(DevPtrs P) {
 // reference's balance cancel pairwise (q_e of cell i equals q_w of cell i+1
 // bit for bit), so only boundary faces are summed.
 template <typename T>
-__global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
-    const int tile = blockIdx.x;
+__device__ __forceinline__ void epilogue_tile(const DevPtrs &P, int tile) {
     const TileDesc td = P.tiles[tile];
     const DomainDesc &D = P.dom[td.dom];
     const ColumnRef cr = column_of(P, tile);
@@ -1059,7 +1138,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
             else if (upd == DHARA_THETA_CONSERVATIVE) th_next = thm + Cm * (xn - xm);
             else th_next = thm;
             v[4] += dz * (th_next - thn) + dz * ssc * dt * thm * (xn - psin);
-            if (D.record_branches) bsig += branch_mix(step_now * 64 + 63, BR_SATURATION, g, band3(xn, 0.0, 1e-9));
+            if (records(D, BR_SATURATION)) bsig += branch_mix(step_now * 64 + 63, BR_SATURATION, g, band3(xn, 0.0, 1e-9));
             if (!(xn == xn)) v[8] = 1.0;
             // boundary faces (Neumann values; bottom/top below)
             double fb = 0.0;
@@ -1085,7 +1164,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
         const double ph = fmax(P.hpoten[cr.c] - qt * dt, 0.0);
         P.ph[cr.c] = ph;
         P.h[cr.c] = ph;
-        if (D.record_branches)
+        if (records(D, BR_PONDCLIP))
             bsig += branch_mix(step_now, BR_PONDCLIP, cr.c,
                                band3(P.hpoten[cr.c], qt * dt, rel_band(P.hpoten[cr.c], qt * dt, 1e-15)));
     }
@@ -1104,10 +1183,53 @@ __global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
         dg.picard_iters_total += pc.iter;
         dg.picard_iters_last = pc.iter;
         if (!pc.converged) dg.picard_nonconverged += 1;
-        if (D.record_branches)
+        if (records(D, BR_PICARD))
             atomicAdd(&dg.branch_sig, branch_mix(pc.step, BR_PICARD, td.dom, (unsigned)pc.iter));
         pc.step += 1;
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
+    epilogue_tile<T>(P, blockIdx.x);
+}
+
+// One whole subsurface step (SubsurfaceFlowModel, src/subsurface.cu:686-847)
+// in one persistent launch: the prologue, up to maxiter Picard iterations of
+// assembly (+ the Dirichlet passes), linear solve and convergence check, and
+// the epilogue, as phases separated by grid barriers.  Each phase runs the same
+// per-tile code as the separate kernels (prologue_tile ... epilogue_tile,
+// krylov_solve) in the same order, so the results are those of the
+// launch-per-kernel sequence bit for bit; the loop ends as soon as every
+// domain's Picard iteration is done.
+template <typename T, int TXC>
+__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F32 : KRYLOV_BLOCKS_F64)
+    k_step(DevPtrs P, int maxiter, int dirichlet) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar[STAGES];
+    constexpr bool DSMEM = sizeof(T) == 4 && KRYLOV_DSMEM_F32;
+    const SolveSmem<T> sm = solve_smem<T, DSMEM>(P, smem_raw, s_bar);
+    StageBars sb{s_bar, 0u, P.barrier, 0u};
+    auto tiles = [&](auto fn) {
+        for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) fn(t);
+    };
+    tiles([&](int t) { prologue_tile(P, t); });
+    if (!grid_sync(P.barrier)) return;
+    for (int m = 0; m < maxiter; ++m) {
+        tiles([&](int t) { assemble_tile<T>(P, t); });
+        if (!grid_sync(P.barrier)) return;
+        if (dirichlet) {
+            tiles([&](int t) { dir_fixed_tile<T>(P, t); });
+            if (!grid_sync(P.barrier)) return;
+            tiles([&](int t) { dir_rows_tile<T>(P, t); });
+            if (!grid_sync(P.barrier)) return;
+        }
+        if (!krylov_solve<T, DSMEM, TXC>(P, sm, sb)) return;
+        tiles([&](int t) { picard_check_tile(P, t); });
+        if (!grid_sync(P.barrier)) return;
+        if (ldcg(&P.gctrl->n_picard) == 0) break;
+    }
+    tiles([&](int t) { epilogue_tile<T>(P, t); });
 }
 
 // Evaluates the closure at psi^n into out: which = 0 theta, 1 K, 2 C.
@@ -1176,16 +1298,41 @@ cudaError_t launch_dirichlet(const DevPtrs &P, const LaunchCfg &L, cudaStream_t 
     return cudaGetLastError();
 }
 
+// The instantiation for the handle's tile shapes: one shape for every domain
+// (L.uniform_tx 32 or 16) or a mix (0).
+template <int TXC>
+const void *krylov_fn(int mixed) {
+    return mixed ? (const void *)k_krylov<float, TXC> : (const void *)k_krylov<double, TXC>;
+}
+template <int TXC>
+const void *step_fn(int mixed) {
+    return mixed ? (const void *)k_step<float, TXC> : (const void *)k_step<double, TXC>;
+}
+const void *krylov_kernel(const LaunchCfg &L, int uniform_tx) {
+    return uniform_tx == TILE_X ? krylov_fn<TILE_X>(L.mixed) : uniform_tx == 16 ? krylov_fn<16>(L.mixed)
+                                                                                : krylov_fn<0>(L.mixed);
+}
+const void *step_kernel(const LaunchCfg &L, int uniform_tx) {
+    return uniform_tx == TILE_X ? step_fn<TILE_X>(L.mixed) : uniform_tx == 16 ? step_fn<16>(L.mixed)
+                                                                              : step_fn<0>(L.mixed);
+}
+
 cudaError_t launch_krylov(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s) {
     DevPtrs args = P;
     void *kargs[] = {&args};
     const int blocks = L.krylov_per_sm * L.sms;
     const int grid = blocks < P.ntiles ? blocks : P.ntiles;
-    if (L.mixed)
-        return cudaLaunchCooperativeKernel((const void *)k_krylov<float>, dim3(grid), dim3(TILE_THREADS),
-                                           kargs, (size_t)L.smem_3d, s);
-    return cudaLaunchCooperativeKernel((const void *)k_krylov<double>, dim3(grid), dim3(TILE_THREADS),
-                                       kargs, (size_t)L.smem_3d, s);
+    return cudaLaunchCooperativeKernel(krylov_kernel(L, L.uniform_tx), dim3(grid), dim3(TILE_THREADS), kargs,
+                                       (size_t)L.smem_3d, s);
+}
+
+cudaError_t launch_step(const DevPtrs &P, const LaunchCfg &L, int maxiter, int dirichlet, cudaStream_t s) {
+    DevPtrs args = P;
+    void *kargs[] = {&args, &maxiter, &dirichlet};
+    const int blocks = (L.krylov_per_sm < L.step_per_sm ? L.krylov_per_sm : L.step_per_sm) * L.sms;
+    const int grid = blocks < P.ntiles ? blocks : P.ntiles;
+    return cudaLaunchCooperativeKernel(step_kernel(L, L.uniform_tx), dim3(grid), dim3(TILE_THREADS), kargs,
+                                       (size_t)L.smem_3d, s);
 }
 
 cudaError_t configure_3d(LaunchCfg &L, int device, int ntiles) {
@@ -1196,17 +1343,28 @@ cudaError_t configure_3d(LaunchCfg &L, int device, int ntiles) {
     const size_t dprime = (L.mixed && KRYLOV_DSMEM_F32) ? elt * (size_t)L.nz_max * TILE_THREADS : 0;
     const size_t stage = L.mixed ? StageSize<float>::bytes() : StageSize<double>::bytes();
     L.smem_3d = (int)(128 + ((dprime + 127) & ~(size_t)127) + stage);
-    const void *fn = L.mixed ? (const void *)k_krylov<float> : (const void *)k_krylov<double>;
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_3d);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, TILE_THREADS, L.smem_3d);
-    if (e != cudaSuccess) return e;
+    // every instantiation (tile shapes 32, 16 and mixed) takes the same shared
+    // memory; the co-resident block counts are the smallest over them
+    int per_sm = 1 << 30, step_sm = 1 << 30;
+    for (int u : {TILE_X, 16, 0}) {
+        for (int fused = 0; fused < 2; ++fused) {
+            const void *fn = fused ? step_kernel(L, u) : krylov_kernel(L, u);
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_3d);
+            if (e != cudaSuccess) return e;
+            int n = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, TILE_THREADS, L.smem_3d);
+            if (e != cudaSuccess) return e;
+            int &acc = fused ? step_sm : per_sm;
+            acc = n < acc ? n : acc;
+        }
+    }
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     L.coop_blocks_3d = per_sm * prop.multiProcessorCount;
     L.sms = prop.multiProcessorCount;
     L.krylov_per_sm_max = per_sm;
     L.krylov_per_sm = per_sm;
+    L.step_per_sm = step_sm < per_sm ? step_sm : per_sm;
+    if (L.step_per_sm < 1) return cudaErrorInvalidConfiguration;
     (void)ntiles;
     return cudaSuccess;
 }

@@ -41,12 +41,15 @@ def gather_diagnostics(local, world):
     return merged
 
 
-def run_sharded(domains, nsteps, rank, world, device=0, graph=True):
+def run_sharded(domains, nsteps, rank, world, device=0, graph=True, autotune=0):
     """Advances this rank's share of `domains` (inputs.Domain objects) for
     nsteps in one handle on `device`; returns this rank's device time in ms
     (CUDA events on the handle's stream), the number of kernel launches it
     made, and the diagnostics of all domains (plus each domain's largest
-    |psi| after the run, "psi_abs_max"), gathered from every rank."""
+    |psi| after the run, "psi_abs_max", and under "launch_config" the
+    schedule used), gathered from every rank.  autotune > 0 first lets
+    dhara_autotune choose the tile shapes and schedules with that many trial
+    steps (the state is restored before the timed run)."""
     import torch
     import dhara_b200 as db
     cells = [d.ncells for d in domains]
@@ -59,6 +62,7 @@ def run_sharded(domains, nsteps, rank, world, device=0, graph=True):
             for j, i in enumerate(mine):
                 s.load(domains[i], j)
             s.prepare()
+            cfg = s.autotune(autotune) if autotune > 0 else s.launch_config()
             stream = torch.cuda.ExternalStream(s.stream, device=device)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -73,6 +77,7 @@ def run_sharded(domains, nsteps, rank, world, device=0, graph=True):
             for j, i in enumerate(mine):
                 local[i] = s.diagnostics(j)
                 local[i]["psi_abs_max"] = float(np.abs(s.download("psi", j)).max())
+                local[i]["launch_config"] = cfg
         finally:
             s.close()
     return ms, launches, gather_diagnostics(local, world)

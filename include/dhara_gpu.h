@@ -105,8 +105,14 @@ typedef struct {
      * the FP64 system's); 1 evaluates the closure in FP32 (faster; the
      * refinement then converges to the FP32-coefficient system). */
     int32_t closure_fp32;
-    /* 1: accumulate dhara_diagnostics.branch_signature (costs a hash and a
-     * warp-aggregated atomic per decision; off by default). */
+    /* Decisions to fold into dhara_diagnostics.branch_signature, a bit mask:
+     * 1 top-flux selection, 2 ponding clip, 4 Manning's wet/slope test,
+     * 8 overland depth clip, 16 saturation (psi >= 0) of every cell at every
+     * closure evaluation, 32 Picard iteration count, 64 overland CG iteration
+     * count (a solve that stops at a different iteration is a different
+     * map); 0 (the default) records nothing.  Each recorded decision costs a hash and a warp-aggregated
+     * atomic.  Saturation is not a switch of the loss (theta and K are
+     * continuous there) but of the closure's formula. */
     int32_t record_branches;
     int32_t reserved_i[5];
     double reserved_d[8];
@@ -253,7 +259,8 @@ int dhara_get_stream(dhara_handle *h, void **stream);
 /* Per-kernel CUDA-event timing (off by default).  kernel: 0 = 3D Krylov solve,
  * 1 = Picard assembly, 2 = Picard check, 3 = step epilogue, 4 = overland solve,
  * 5 = overland set-up/finish, 6 = step prologue, 7 = the adjoint's own kernels
- * (its linear solves count under 0 and 4). */
+ * (its linear solves count under 0 and 4), 8 = the fused subsurface step
+ * (dhara_launch_config.fused_step: kernels 0-3 and 6 run inside it). */
 int dhara_set_kernel_timing(dhara_handle *h, int enable);
 int dhara_get_kernel_timing(dhara_handle *h, int kernel, int64_t *launches, double *total_ms);
 int dhara_reset_kernel_timing(dhara_handle *h);
@@ -264,22 +271,34 @@ int dhara_get_launch_count(dhara_handle *h, int64_t *count);
 int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations);
 
 /* ---- block schedules ---------------------------------------------------------
- * The persistent solvers' block schedules: how many co-resident blocks per SM
- * the 3D Krylov solve launches (its tiles are strided over them), and whether
- * the overland solve keeps each segment's vectors in shared memory (one block
- * per segment, when they fit) or streams them with a given number of blocks
- * per SM.  dhara_autotune times the candidates on this handle's own data --
+ * The persistent solvers' block schedules and the 3D kernels' tile shape: the
+ * column tiles every 3D kernel works on (32 x 4 or 16 x 8 columns of 128
+ * threads, per domain or for all), how many co-resident blocks per SM the 3D
+ * Krylov solve launches (its tiles are strided over them), and whether the
+ * overland solve keeps each segment's vectors in shared memory (one block per
+ * segment, when they fit) or streams them with a given number of blocks per
+ * SM.  dhara_autotune times the candidates on this handle's own data --
  * trial_steps steps per candidate from the current state, which it restores
  * afterwards -- and keeps the fastest; *chosen (may be NULL) receives the
- * result.  Defaults: the most blocks per SM that fit, overland resident when
- * possible. */
+ * result.  Defaults: tiles per domain, the most blocks per SM that fit,
+ * overland resident when possible.  Results agree across schedules to
+ * rounding (reductions run over tiles in a fixed order; a different tile
+ * shape groups the sums differently), and bit for bit across block counts. */
 typedef struct {
     int32_t krylov_blocks_per_sm;
     int32_t overland_resident;
     int32_t overland_blocks_per_sm;
-    int32_t pad;
+    /* column tiles of the 3D kernels: 1 = 32 x 4 for every domain, 2 = 16 x 8,
+     * 0 = per domain whichever needs fewer tiles (fewer idle threads in the
+     * ragged tiles of narrow domains; 32 x 4 on a tie) -- the default */
+    int32_t tile_shape;
     double krylov_ms;     /* per trial step of the chosen schedule (autotune only) */
     double overland_ms;
+    /* 1: each subsurface step is one persistent launch (prologue, every Picard
+     * iteration's assembly, solve and check, epilogue); 0: a launch per kernel
+     * (the default; per-kernel timing then names every phase) */
+    int32_t fused_step;
+    int32_t pad;
 } dhara_launch_config;
 
 int dhara_autotune(dhara_handle *h, int trial_steps, dhara_launch_config *chosen);

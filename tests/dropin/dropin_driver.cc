@@ -126,6 +126,32 @@ int main(int argc, char **argv) {
     save(dir + "/out_ph.bin", ph);
     save(dir + "/out_H.bin", H);
     save(dir + "/out_mb.bin", mb);
+    // the reference's result files after the last step (SaveModelResults,
+    // SaveResultEntirePeriod), from the structs as the reference's loop leaves them
+    {
+        ProjectClass proj = {};
+        proj.folderoutput = dir.c_str();
+        proj.olfoutput = "olf";
+        proj.ssfoutput = "ssf";
+        proj.ssf1doutput = "ssf1d";
+        proj.statoutput = "stat";
+        proj.saveolf = proj.savessf = proj.savestat = 1;
+        proj.saveinterval = 1;
+        proj.num_steps = nsteps;
+        std::vector<double> elev(C), depth(C), psi_col((size_t)nsteps * g.z, 0.0), theta_col((size_t)nsteps * g.z, 0.0);
+        std::vector<double> psi_host(N), theta_host(N);
+        oh.waterelev = elev.data();
+        oh.waterdepth = depth.data();
+        // SaveModelResults copies into the host struct's psiout/thetaout
+        // (src/io.cc:889-894), which the reference allocates beside the
+        // device struct's (src/numerical.cc:38-192)
+        sh.psiout = psi_host.data();
+        sh.thetaout = theta_host.data();
+        sh.psi_col = psi_col.data();
+        sh.theta_col = theta_col.data();
+        SaveModelResults(&proj, &oh, &od, &sh, &sd, g, nsteps);
+        SaveResultEntirePeriod(&proj, &sh, g);
+    }
     dhara_destroy(solver);
     printf("dropin ok\n");
     return 0;

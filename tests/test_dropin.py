@@ -47,6 +47,15 @@ def test_dropin_matches_oracle(gpu):
         out = subprocess.run([exe, tmp, str(nsteps)], capture_output=True, text=True, timeout=300)
         assert out.returncode == 0, out.stderr
         got = {k: np.fromfile(os.path.join(tmp, f"out_{k}.bin")) for k in ("psi", "theta", "ph", "H", "mb")}
+        # SaveModelResults / SaveResultEntirePeriod wrote the reference's files
+        from scipy.io import netcdf_file
+        with netcdf_file(os.path.join(tmp, f"ssf_{nsteps}.nc"), "r", mmap=False) as f:
+            assert np.array_equal(f.variables["pressure_head"][:].reshape(-1), got["psi"])
+            assert np.array_equal(f.variables["moisture"][:].reshape(-1), got["theta"])
+        with netcdf_file(os.path.join(tmp, f"olf_{nsteps}.nc"), "r", mmap=False) as f:
+            assert np.array_equal(f.variables["water_elevation"][:].reshape(-1), got["H"])
+        with netcdf_file(os.path.join(tmp, "ssf1d.nc"), "r", mmap=False) as f:
+            assert np.array_equal(f.variables["mb_subsurfaceW"][:], got["mb"])
     # the reference algorithm (FP64 oracle, converged 3D solves)
     o, od, _ = oracle.run(d, nsteps, solver3d=oracle.SOLVER_CG)
     assert rel_err(got["psi"], o["psi"]) < 1e-7

@@ -52,3 +52,42 @@ def test_autotune_restores_state(gpu):
     assert s.launch_config()["krylov_blocks_per_sm"] == chosen["krylov_blocks_per_sm"]
     s.step(2)
     s.close()
+
+
+@pytest.mark.parametrize("prec", [db.FP64, db.MIXED])
+def test_tile_shapes_agree(gpu, prec):
+    """32 x 4 and 16 x 8 tiles group the reductions differently, so results
+    agree to the solver tolerance rather than bit for bit; the per-domain
+    choice (this 40 x 36 surface needs 15 tiles of 16 x 8 against 18 of
+    32 x 4) is one of the two."""
+    from conftest import rel_err
+    d = inputs.make_domain(40, 36, 12, seed=21, rain_mm_per_h=40.0, nsteps=6, krylov_tol=1e-12,
+                           krylov_maxiter=2000, precision=prec)
+    out = {}
+    for shape in (1, 2, 0):
+        s = db.Solver(d.params)
+        s.load(d)
+        s.prepare()
+        cfg = s.launch_config()
+        s.set_launch_config(cfg["krylov_blocks_per_sm"], cfg["overland_resident"], cfg["overland_blocks_per_sm"],
+                            shape)
+        assert s.launch_config()["tile_shape"] == shape
+        s.step(4)
+        out[shape] = {k: s.download(k) for k in ("psi", "theta", "ponding", "waterelev")}
+        s.close()
+    for k in out[1]:
+        assert rel_err(out[2][k], out[1][k]) < 1e-8, k
+        assert np.array_equal(out[0][k], out[2][k]), k
+
+
+def test_autotune_picks_a_tile_shape(gpu):
+    d = domain()
+    s = db.Solver(d.params)
+    s.load(d)
+    s.prepare()
+    chosen = s.autotune(1)
+    assert chosen["tile_shape"] in (0, 1, 2)
+    assert s.launch_config()["tile_shape"] == chosen["tile_shape"]
+    s.step(2)
+    assert s.diagnostics()["nonfinite"] == 0
+    s.close()

@@ -64,3 +64,36 @@ def test_snapshot_overlaps_next_steps(gpu):
     np.testing.assert_array_equal(bufs[0]["water_depth"], want["waterdepth"])
     assert not np.array_equal(bufs[1]["pressure_head"], want["psi"])
     s.close()
+
+
+def test_netcdf_files_from_a_handle(gpu, tmp_path):
+    """The reference's result files (SaveModelResults / SaveResultEntirePeriod,
+    src/io.cc:854-996) written from a handle, read back with scipy's NetCDF
+    reader: the current state and the statistics kept on the device."""
+    netcdf = pytest.importorskip("scipy.io").netcdf_file
+    d = small()
+    p = d.params
+    s = db.Solver(p)
+    s.load(d)
+    s.enable_statistics(8)
+    s.prepare()
+    s.step(3)
+    s.synchronize()
+    f2, f3 = str(tmp_path / "olf_3.nc"), str(tmp_path / "ssf_3.nc")
+    f1, fs = str(tmp_path / "ssf1d.nc"), str(tmp_path / "stat.nc")
+    s.save_netcdf(f2, f3)
+    s.save_netcdf_statistics(f1, fs)
+    state = {k: s.download(k) for k in ("waterelev", "waterdepth", "psi", "theta")}
+    st = s.statistics()
+    s.close()
+    with netcdf(f2, "r", mmap=False) as f:
+        assert np.array_equal(f.variables["water_elevation"][:], state["waterelev"].reshape(p.ny, p.nx))
+        assert np.array_equal(f.variables["water_depth"][:], state["waterdepth"].reshape(p.ny, p.nx))
+    with netcdf(f3, "r", mmap=False) as f:
+        assert np.array_equal(f.variables["pressure_head"][:], state["psi"].reshape(p.nz, p.ny, p.nx))
+        assert np.array_equal(f.variables["moisture"][:], state["theta"].reshape(p.nz, p.ny, p.nx))
+    with netcdf(f1, "r", mmap=False) as f:
+        assert np.array_equal(f.variables["mb_subsurfaceW"][:], st["mb_subsurfaceW"])
+    with netcdf(fs, "r", mmap=False) as f:
+        assert np.array_equal(f.variables["pressure_mean"][:], st["pressure_sum"])
+        assert np.array_equal(f.variables["moisture_mean"][:], st["moisture_sum"])
