@@ -48,7 +48,7 @@ class Params(ct.Structure):
         ("krylov_maxiter", ct.c_int32), ("theta_update", ct.c_int32), ("krylov_tol", ct.c_double),
         ("overland_maxiter", ct.c_int32), ("precision", ct.c_int32), ("overland_tol", ct.c_double),
         ("inner_tol", ct.c_double), ("inner_maxiter", ct.c_int32), ("closure_fp32", ct.c_int32),
-        ("record_branches", ct.c_int32), ("reserved_i", ct.c_int32 * 5), ("reserved_d", ct.c_double * 8),
+        ("record_branches", ct.c_int32), ("overland_solver", ct.c_int32), ("reserved_i", ct.c_int32 * 4), ("reserved_d", ct.c_double * 8),
     ]
 
 

@@ -141,6 +141,8 @@ int validate(const dhara_params &p, int d) {
         return fail(DHARA_ERR_INVALID, "domain %d: unknown precision %d", d, p.precision);
     if (!(p.krylov_tol > 0) || !(p.overland_tol > 0) || !(p.picard_tol > 0))
         return fail(DHARA_ERR_INVALID, "domain %d: tolerances must be > 0", d);
+    if (p.overland_solver < 0 || p.overland_solver > 1)
+        return fail(DHARA_ERR_INVALID, "domain %d: unknown overland_solver %d", d, p.overland_solver);
     return DHARA_OK;
 }
 
@@ -600,6 +602,8 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         if (rc) return rc;
         if (params[d].precision != params[0].precision)
             return fail(DHARA_ERR_INVALID, "all domains of a handle must share one precision");
+        if (params[d].overland_solver != params[0].overland_solver)
+            return fail(DHARA_ERR_INVALID, "all domains of a handle must share one overland solver");
     }
     int ndev = 0;
     CK(cudaGetDeviceCount(&ndev));
@@ -697,6 +701,22 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
                        &P.ktop, &P.bcqb, &P.olf_b, &P.olf_r, &P.olf_p0, &P.olf_p1, &P.olf_z, &P.olf_w,
                        &P.olf_s, &P.olf_p})
         rc |= dalloc(h, q, C);
+    // multigrid hierarchy of the overland solve
+    std::vector<MgDom> mgd;
+    std::vector<MgChunk> mgc;
+    int lchunk[MG_MAXLEV + 2];
+    int mg_lg = 0;
+    long long mg_nc = 0;
+    mg_plan(h->hdom, mgd, mgc, lchunk, mg_lg, mg_nc);
+    MgDom *d_mgd = nullptr;
+    MgChunk *d_mgc = nullptr;
+    const int nchunk0 = lchunk[1] - lchunk[0];
+    rc |= dalloc(h, &d_mgd, ndomains);
+    rc |= dalloc(h, &d_mgc, std::max<size_t>(mgc.size(), 1));
+    rc |= dalloc(h, &P.mg_a, 5 * (size_t)std::max(mg_nc, 1LL));
+    for (double **q : {&P.mg_w, &P.mg_b, &P.mg_x, &P.mg_t}) rc |= dalloc(h, q, (size_t)std::max(mg_nc, 1LL));
+    rc |= dalloc(h, &P.mg_part, 5 * (size_t)std::max(nchunk0, 1));
+    rc |= dalloc(h, &P.mgctl, ndomains);
     OlfSeg *d_oseg = nullptr;
     rc |= dalloc(h, &d_oseg, h->hsegs.size());
     rc |= dalloc(h, &P.osst, h->hsegs.size());
@@ -734,6 +754,12 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     P.tiles = d_tiles;
     P.oseg = d_oseg;
     P.nseg = (int)h->hsegs.size();
+    P.mgd = d_mgd;
+    P.mgc = d_mgc;
+    std::memcpy(P.mg_lchunk, lchunk, sizeof(lchunk));
+    P.mg_lg = mg_lg;
+    P.mg_nchunk0 = nchunk0;
+    P.mg_nc = mg_nc;
     P.ntiles = (int)h->htiles.size();
     P.ndom = ndomains;
     P.smem_nz = h->nz_max;
@@ -758,6 +784,14 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         e = cudaMemcpyAsync(d_oseg, h->hsegs.data(), sizeof(OlfSeg) * h->hsegs.size(), cudaMemcpyHostToDevice,
                             h->stream);
     e = e ? e : zero(P.olf_k, 4 * C * 8);
+    e = e ? e : zero(P.mgctl, ndomains * sizeof(MgCtrl));
+    e = e ? e : zero(P.mg_part, 5 * (size_t)std::max(nchunk0, 1) * 8);
+    for (double *q : {P.mg_a, P.mg_w, P.mg_b, P.mg_x, P.mg_t})
+        e = e ? e : zero(q, (q == P.mg_a ? 5 : 1) * (size_t)std::max(mg_nc, 1LL) * 8);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_mgd, mgd.data(), sizeof(MgDom) * mgd.size(), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && !mgc.empty())
+        e = cudaMemcpyAsync(d_mgc, mgc.data(), sizeof(MgChunk) * mgc.size(), cudaMemcpyHostToDevice, h->stream);
     e = e ? e : zero(P.bcqw, (size_t)h->WEtot * 8);
     e = e ? e : zero(P.bcqe, (size_t)h->WEtot * 8);
     e = e ? e : zero(P.bcqs, (size_t)h->SNtot * 8);
@@ -791,8 +825,10 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
 
     h->L.nz_max = h->nz_max;
     h->L.mixed = h->mixed;
+    h->L.olf_mg = params[0].overland_solver == 0 ? 1 : 0;
     e = configure_3d(h->L, device, P.ntiles);
     if (e == cudaSuccess) e = configure_2d(h->L, device);
+    if (e == cudaSuccess) e = configure_mg(h->L, device);
     if (e != cudaSuccess) return bail(fail(DHARA_ERR_CUDA, "kernel configuration: %s", cudaGetErrorString(e)));
     *out = h;
     return DHARA_OK;
@@ -1696,16 +1732,18 @@ int dhara_autotune(dhara_handle *h, int trial_steps, dhara_launch_config *chosen
         if (!rc && ms < best_kms) { best_kms = ms; best_k = b; }
     }
     L.krylov_per_sm = best_k;
-    // overland: resident (when the segments fit) or streaming with b blocks per SM
+    // overland (the Jacobi solver): resident (when the segments fit) or
+    // streaming with b blocks per SM; the multigrid solve has one schedule
     int best_res = L.olf_allow_resident, best_ob = L.olf_stream_per_sm;
     double best_oms = 1e300;
-    if (!rc && h->P.nseg <= L.olf_res_blocks) {
+    if (L.olf_mg && !rc) rc = trial(KT_OLF_SOLVE, &best_oms);
+    if (!L.olf_mg && !rc && h->P.nseg <= L.olf_res_blocks) {
         L.olf_allow_resident = 1;
         double ms = 0;
         rc = trial(KT_OLF_SOLVE, &ms);
         if (!rc && ms < best_oms) { best_oms = ms; best_res = 1; }
     }
-    for (int b = 1; b <= L.olf_stream_per_sm_max && !rc; ++b) {
+    for (int b = 1; b <= L.olf_stream_per_sm_max && !rc && !L.olf_mg; ++b) {
         L.olf_allow_resident = 0;
         L.olf_stream_per_sm = b;
         double ms = 0;

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -142,6 +143,30 @@ struct OlfSegState {
     int iter, active;
 };
 
+// Multigrid hierarchy of the overland solve (overland_mg.cu).  Level 0 is a
+// domain's interior surface grid (the fixed ring eliminated); each coarser
+// level halves every dimension that still has at least 3 points, vertex-
+// centred (coarse point I sits on fine point 2I+1), down to at most 2 x 2.
+#define MG_MAXLEV 16
+#define MG_BLOCK_PTS 4096    // levels of at most this many points run in the domain's own block
+#define MG_COARSE_SWEEPS 7   // smoothing sweeps on the coarsest level (odd: the result ends in t)
+struct MgDom {
+    int nlev;                      // levels; 0 when the domain has no interior cell
+    int lc;                        // first level run by the domain's block (levels lc .. nlev-1)
+    int nx;                        // surface row length (level 0 indexing)
+    int c0_first, c0_count;        // the domain's level-0 chunks (CG partial sums)
+    int m[MG_MAXLEV], n[MG_MAXLEV];             // points per level in x and y
+    unsigned char hx[MG_MAXLEV], hy[MG_MAXLEV]; // level l+1 halves x (y) of level l
+    long long off[MG_MAXLEV];      // level 0: the domain's surface offset; else first coarse point
+};
+// A run of up to OLF_THREADS consecutive points of one level of one domain.
+struct MgChunk {
+    int dom, lev, first, count;
+};
+struct MgCtrl {
+    int active, pad;
+};
+
 // Diagnostics accumulated on the device (copied into dhara_diagnostics).
 struct DevDiag {
     long long picard_iters_total, krylov_iters_total, refine_iters_total, overland_iters_total;
@@ -199,6 +224,17 @@ struct DevPtrs {
     OlfSegState *osst;   // [nseg]
     double *olf_part;    // [2][3][nseg] recurrence sums + [nseg] ||b||^2 partials
     int nseg, pad_seg;
+    // multigrid-preconditioned overland CG (overland_mg.cu)
+    const MgDom *mgd;    // [ndom]
+    const MgChunk *mgc;  // chunk lists: level l's at mg_lchunk[l] .. mg_lchunk[l+1]-1
+    int mg_lchunk[MG_MAXLEV + 2];
+    int mg_lg;           // levels run as grid phases: the largest lc of any domain
+    int mg_nchunk0;      // level-0 chunks (every domain with an interior)
+    long long mg_nc;     // coarse points of all domains and levels
+    double *mg_a;        // [5][mg_nc]: C, E, N, NE, NW of every coarse row
+    double *mg_w, *mg_b, *mg_x, *mg_t;  // [mg_nc] 1/smoother weight, rhs, pre- and post-smoothed
+    double *mg_part;     // [5][mg_nchunk0] chunk partials: p.q, r.r, r.z (two slots), b.b
+    MgCtrl *mgctl;       // [ndom]
     // faces
     double *bcqw, *bcqe, *bcqs, *bcqn;
     // Dirichlet faces: 1 where the face is type 0, and the fixed heads
@@ -238,6 +274,8 @@ struct LaunchCfg {
     int step_per_sm;      // co-resident blocks per SM of the fused step kernel
     int fused_step;       // run the subsurface step as one launch (k_step)
     int uniform_tx;       // the tile width shared by every domain (32 or 16), 0 if they differ
+    int olf_mg;           // overland solve: 1 multigrid-preconditioned CG, 0 pipelined Jacobi-PCG
+    int mg_blocks;        // co-resident blocks of the multigrid solve
 };
 
 cudaError_t launch_psi_from_theta(const DevPtrs &P, cudaStream_t s);
@@ -255,6 +293,12 @@ cudaError_t launch_eval_fields(const DevPtrs &P, int which, double *out, cudaStr
 cudaError_t launch_overland_setup(const DevPtrs &P, long long ctot, cudaStream_t s);
 cudaError_t launch_overland_solve(const DevPtrs &P, const LaunchCfg &L, long long ctot, cudaStream_t s);
 cudaError_t launch_overland_finish(const DevPtrs &P, long long ctot, cudaStream_t s);
+// Multigrid hierarchy of the overland solve for the given domains: per-domain
+// levels, the chunk lists (level by level) and the number of coarse points.
+cudaError_t launch_overland_mg(const DevPtrs &P, const LaunchCfg &L, long long ctot, cudaStream_t s);
+void mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::vector<MgChunk> &chunks,
+             int (&lchunk)[MG_MAXLEV + 2], int &lg, long long &nc);
+cudaError_t configure_mg(LaunchCfg &L, int device);
 // Discrete adjoint (adjoint.cu).  Tape of one checkpoint segment, the
 // carried adjoint state and the gradient accumulators; 3D arrays in the
 // pitched layout of the handle, 2D arrays dense.

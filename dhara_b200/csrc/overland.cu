@@ -12,11 +12,7 @@
 // same solution as the reference's, and its interior block is symmetric, so
 // Jacobi-preconditioned CG applies.  Interior rows use the reference's
 // row-owned conductances kw, ke, ks, kn exactly.
-#include "device_common.cuh"
-
-__device__ __forceinline__ bool is_ring(int i, int j, int nx, int ny) {
-    return i == 0 || j == 0 || i == nx - 1 || j == ny - 1;
-}
+#include "overland_common.cuh"
 
 // Manning conductance of one face (src/overland.cu:279-297 and the three
 // analogous blocks): the depth test is upwinded on the water elevation.
@@ -135,44 +131,6 @@ __device__ __forceinline__ double olf_apply(const OlfRow &w, const ColumnRef &cr
 // (blocks loop over segments); both do the same arithmetic in the same order,
 // so their results agree bit for bit.
 
-template <int NV>
-__device__ __forceinline__ void olf_block_sum(double (&v)[NV]) {
-    __shared__ double s_w[NV][OLF_THREADS / 32];
-    __shared__ double s_out[NV];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-        double a = v[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-        if (lane == 0) s_w[i][warp] = a;
-    }
-    __syncthreads();
-    if (threadIdx.x < NV) {
-        double a = 0.0;
-#pragma unroll
-        for (int w = 0; w < OLF_THREADS / 32; ++w) a += s_w[threadIdx.x][w];
-        s_out[threadIdx.x] = a;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < NV; ++i) v[i] = s_out[i];
-    __syncthreads();
-}
-
-// Domain totals of per-segment partials (component-major: part[i*nseg + s]).
-template <int NV>
-__device__ __forceinline__ void olf_domain_sum(const double *part, int nseg_tot, int first, int nseg,
-                                               double (&v)[NV]) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) v[i] = 0.0;
-    for (int k = threadIdx.x; k < nseg; k += OLF_THREADS) {
-#pragma unroll
-        for (int i = 0; i < NV; ++i) v[i] += __ldcg(&part[(size_t)i * nseg_tot + first + k]);
-    }
-    olf_block_sum<NV>(v);
-}
-
 struct OlfCell {
     long long c;
     int nx;
@@ -188,37 +146,6 @@ __device__ __forceinline__ OlfCell olf_cell(const OlfSeg &sg, const DomainDesc &
     q.nx = D.nx;
     q.ring = is_ring(i, j, D.nx, D.ny);
     return q;
-}
-
-// 5-point product of the interior row at c: diag*v_c - sum of the scaled
-// conductances times the neighbours (row-owned kw, ke, ks, kn as the
-// reference's SetUpLinearSystemsOverland builds them).
-struct OlfCoef {
-    double cw, ce, cs, cn, dg;
-};
-
-__device__ __forceinline__ OlfCoef olf_coef(const DevPtrs &P, const DomainDesc &D, long long c, long long ctot) {
-    const double cx = D.dt / (D.dx * D.dx), cy = D.dt / (D.dy * D.dy);
-    OlfCoef k;
-    k.cw = cx * P.olf_k[0 * ctot + c];
-    k.ce = cx * P.olf_k[1 * ctot + c];
-    k.cs = cy * P.olf_k[2 * ctot + c];
-    k.cn = cy * P.olf_k[3 * ctot + c];
-    k.dg = 1.0 + (k.ce + k.cw) + (k.cn + k.cs);
-    return k;
-}
-
-__device__ __forceinline__ double olf_av4(const OlfCoef &k, double vc, double vw, double ve, double vs, double vn) {
-    return k.dg * vc - ((k.ce * ve + k.cw * vw) + (k.cn * vn + k.cs * vs));
-}
-
-template <bool CG>
-__device__ __forceinline__ double olf_av(const OlfCoef &k, const double *v, long long c, int nx, double vc) {
-    const double vw = CG ? __ldcg(v + c - 1) : v[c - 1];
-    const double ve = CG ? __ldcg(v + c + 1) : v[c + 1];
-    const double vs = CG ? __ldcg(v + c - nx) : v[c - nx];
-    const double vn = CG ? __ldcg(v + c + nx) : v[c + nx];
-    return olf_av4(k, vc, vw, ve, vs, vn);
 }
 
 // Vectors of one interior row carried by the pipelined recurrence.
@@ -706,6 +633,7 @@ cudaError_t launch_overland_solve(const DevPtrs &P, const LaunchCfg &L, long lon
     DevPtrs args = P;
     long long c = ctot;
     void *kargs[] = {&args, &c};
+    if (L.olf_mg) return launch_overland_mg(P, L, ctot, s);
     if (L.olf_allow_resident && P.nseg <= L.olf_res_blocks)
         return cudaLaunchCooperativeKernel((const void *)k_olf_pcg_res, dim3(P.nseg), dim3(OLF_THREADS), kargs,
                                            OLF_RES_SMEM, s);

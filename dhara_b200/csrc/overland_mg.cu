@@ -1,0 +1,676 @@
+// overland_mg.cu -- the overland solve (the reference's CUSP CG on the
+// 5-point system, src/overland.cu:410-411) as conjugate gradients
+// preconditioned by one geometric multigrid V-cycle per iteration.
+//
+// Why: over ponded, flat ground Manning's conductance h^(5/3) / (n sqrt S)
+// makes the system I + dt L_K nearly singular (dt K / dx^2 reaches 1e4-1e5
+// over a pool), and point-Jacobi-preconditioned CG needs thousands of
+// iterations for a 1e-12 relative residual (1,400-2,100 on 256 x 256 storm
+// surfaces, growing with the grid); the reference's 100-iteration cap stops
+// far from the solution.  A V-cycle removes the smooth error that point
+// smoothing cannot: 60-90 iterations on the same systems, nearly independent
+// of the grid size.
+//
+// Hierarchy (per domain, planned on the host by mg_plan): level 0 is the
+// interior of the surface grid (the fixed ring is eliminated, as in the
+// Jacobi solver); level l+1 halves every dimension of level l that has at
+// least 3 points, vertex-centred (coarse point I sits on fine point 2I+1), so
+// the coarsest level has at most 2 x 2 points.  Prolongation P is bilinear
+// (weights 1 and 1/2 per dimension), restriction is P^T, and the coarse
+// operators are the Galerkin products A_{l+1} = P^T A_l P, recomputed for
+// every solve.  They are 9-point; each row stores C, E, N, NE and NW, and a
+// row's W, S, SW and SE are its neighbours' E, N, NE and NW, so every stored
+// operator is symmetric bit for bit.  The smoother is Jacobi with per-row
+// weights w_i = max(a_ii / 0.8, 0.55 sum_j |a_ij|) (weighted Jacobi at 0.8
+// wherever that is safe): 2W - A is then diagonally dominant, every sweep is
+// convergent, and the V(1,1) cycle -- pre-smoothing from zero, coarse
+// correction, post-smoothing, and MG_COARSE_SWEEPS sweeps on the coarsest
+// level -- is a fixed symmetric positive definite operator, as CG needs.
+//
+// Schedule: one persistent cooperative launch per solve for all domains.
+// Levels with more than MG_BLOCK_PTS points run as grid phases over chunks of
+// OLF_THREADS points, one grid barrier each; a domain's smaller levels run in
+// one block with block barriers.  The residual is fused into the restriction
+// and the prolongation into the post-smoothing (each point recomputes the few
+// neighbour values it needs), so a grid level costs one barrier on the way
+// down and one on the way up; and with q = A z + beta q the CG updates p and q
+// in one phase.  An iteration on a 512 x 512 surface is nine grid barriers.
+// Every reduction runs over chunks in a fixed order, so results do not depend
+// on the block count.
+#include <algorithm>
+#include <cstring>
+
+#include "overland_common.cuh"
+
+namespace {
+
+// chunk partial slots: p.q, r.r, r.z (iteration parity 0 / 1), b.b
+enum { MP_PQ = 0, MP_RR = 1, MP_RZ = 2, MP_BB = 4 };
+
+// ---------------------------------------------------------------- geometry
+// Level l of one domain: its points, where its arrays start, how rows index.
+struct Lvl {
+    int m, n;
+    int nx;          // level 0: the surface row length
+    bool fine;       // level 0: vectors live in the surface arrays
+    long long base;  // level 0: the domain's surface offset; else the first coarse point
+    __device__ __forceinline__ long long at(int i, int j) const {
+        return fine ? base + (long long)(j + 1) * nx + (i + 1) : base + (long long)j * m + i;
+    }
+};
+
+__device__ __forceinline__ Lvl level(const MgDom &g, int l) {
+    return Lvl{g.m[l], g.n[l], g.nx, l == 0, g.off[l]};
+}
+
+// Vectors of a level: right-hand side, pre-smoothed and post-smoothed
+// (final) solution.  Level 0 uses the CG's residual, z and w arrays.
+struct LvlVec {
+    const double *b;
+    double *x, *t;
+};
+
+__device__ __forceinline__ LvlVec vectors(const DevPtrs &P, int l) {
+    if (l == 0) return LvlVec{P.olf_r, P.olf_z, P.olf_w};
+    return LvlVec{P.mg_b, P.mg_x, P.mg_t};
+}
+
+// Parents of fine index i (level l) on level l+1 along one dimension: the
+// coarse point on it (weight 1) or the two beside it (1/2 each, those inside
+// the level); identity where the dimension is not halved.
+__device__ __forceinline__ int parents(int i, bool halves, int mc, int (&I)[2], double (&w)[2]) {
+    if (!halves) {
+        I[0] = i;
+        w[0] = 1.0;
+        return 1;
+    }
+    if (i & 1) {
+        I[0] = (i - 1) >> 1;
+        w[0] = 1.0;
+        return 1;
+    }
+    int k = 0;
+    if (i >= 2) { I[k] = (i >> 1) - 1; w[k] = 0.5; ++k; }
+    if ((i >> 1) < mc) { I[k] = i >> 1; w[k] = 0.5; ++k; }
+    return k;
+}
+
+// Children of coarse index I (level l+1) on level l along one dimension:
+// 2I, 2I+1, 2I+2 with weights 1/2, 1, 1/2 (those inside the level).
+__device__ __forceinline__ int children(int I, bool halves, int mf, int (&f)[3], double (&w)[3]) {
+    if (!halves) {
+        f[0] = I;
+        w[0] = 1.0;
+        return 1;
+    }
+    int k = 0;
+    f[k] = 2 * I; w[k] = 0.5; ++k;
+    f[k] = 2 * I + 1; w[k] = 1.0; ++k;
+    if (2 * I + 2 < mf) { f[k] = 2 * I + 2; w[k] = 0.5; ++k; }
+    return k;
+}
+
+// Row (i, j) of level l's operator as a 3 x 3 stencil a[dj+1][di+1]; zero
+// where the neighbour is outside the level.  Level 0 is the reference's
+// 5-point interior row (row-owned conductances, ring couplings eliminated).
+struct Row9 {
+    double a[3][3];
+};
+
+__device__ __forceinline__ Row9 row_of(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g,
+                                       int l, const Lvl &v, int i, int j) {
+    Row9 r;
+#pragma unroll
+    for (int y = 0; y < 3; ++y)
+#pragma unroll
+        for (int x = 0; x < 3; ++x) r.a[y][x] = 0.0;
+    if (l == 0) {
+        const OlfCoef cf = olf_coef(P, D, v.at(i, j), ctot);
+        r.a[1][1] = cf.dg;
+        if (i > 0) r.a[1][0] = -cf.cw;
+        if (i < v.m - 1) r.a[1][2] = -cf.ce;
+        if (j > 0) r.a[0][1] = -cf.cs;
+        if (j < v.n - 1) r.a[2][1] = -cf.cn;
+        return r;
+    }
+    const long long nc = P.mg_nc;
+    const double *A = P.mg_a;
+    auto e = [&](int k, int ii, int jj) { return __ldcg(A + (size_t)k * nc + v.at(ii, jj)); };
+    const bool w = i > 0, ea = i < v.m - 1, s = j > 0, no = j < v.n - 1;
+    r.a[1][1] = e(0, i, j);
+    if (ea) r.a[1][2] = e(1, i, j);
+    if (w) r.a[1][0] = e(1, i - 1, j);
+    if (no) r.a[2][1] = e(2, i, j);
+    if (s) r.a[0][1] = e(2, i, j - 1);
+    if (ea && no) r.a[2][2] = e(3, i, j);
+    if (w && s) r.a[0][0] = e(3, i - 1, j - 1);
+    if (w && no) r.a[2][0] = e(4, i, j);          // NW couples (i, j) to (i-1, j+1)
+    if (ea && s) r.a[0][2] = e(4, i + 1, j - 1);  // SE is (i+1, j-1)'s NW
+    return r;
+}
+
+// (A v)(i, j) on level l.
+__device__ __forceinline__ double apply_row(const Row9 &r, const double *x, const Lvl &v, int i, int j) {
+    double s = 0.0;
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+            const double a = r.a[dy + 1][dx + 1];
+            if (a != 0.0) s += a * __ldcg(x + v.at(i + dx, j + dy));
+        }
+    return s;
+}
+
+// 1 / smoother weight of row (i, j).
+__device__ __forceinline__ double smoother_inv(const Row9 &r) {
+    double l1 = 0.0;
+#pragma unroll
+    for (int y = 0; y < 3; ++y)
+#pragma unroll
+        for (int x = 0; x < 3; ++x) l1 += fabs(r.a[y][x]);
+    return 1.0 / fmax(r.a[1][1] / 0.8, 0.55 * l1);
+}
+
+__device__ __forceinline__ double winv_at(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g,
+                                          int l, const Lvl &v, int i, int j) {
+    if (l == 0) return 0.8 / olf_coef(P, D, v.at(i, j), ctot).dg;  // the weight is a_ii/0.8 on the M-matrix
+    return __ldcg(P.mg_w + v.at(i, j));
+}
+
+// ---------------------------------------------------------- point kernels
+// Galerkin row (I, J) of level l+1: C, E, N, NE and NW of P^T A_l P.
+__device__ void galerkin_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l,
+                               int I, int J) {
+    const Lvl f = level(g, l), c = level(g, l + 1);
+    const bool hx = g.hx[l], hy = g.hy[l];
+    int fx[3], fy[3];
+    double wx[3], wy[3];
+    const int nfx = children(I, hx, f.m, fx, wx), nfy = children(J, hy, f.n, fy, wy);
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int b = 0; b < nfy; ++b)
+        for (int a = 0; a < nfx; ++a) {
+            const double wf = wx[a] * wy[b];
+            const Row9 r = row_of(P, D, ctot, g, l, f, fx[a], fy[b]);
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const double av = r.a[dy + 1][dx + 1];
+                    if (av == 0.0) continue;
+                    int px[2], py[2];
+                    double ux[2], uy[2];
+                    const int npx = parents(fx[a] + dx, hx, c.m, px, ux);
+                    const int npy = parents(fy[b] + dy, hy, c.n, py, uy);
+                    for (int q = 0; q < npy; ++q)
+                        for (int p = 0; p < npx; ++p) {
+                            const int di = px[p] - I, dj = py[q] - J;
+                            const int k = (di == 0 && dj == 0) ? 0 : (di == 1 && dj == 0) ? 1
+                                        : (di == 0 && dj == 1)   ? 2 : (di == 1 && dj == 1) ? 3
+                                        : (di == -1 && dj == 1)  ? 4 : -1;
+                            if (k >= 0) acc[k] += wf * av * ux[p] * uy[q];
+                        }
+                }
+        }
+    const long long at = c.at(I, J);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) P.mg_a[(size_t)k * P.mg_nc + at] = acc[k];
+}
+
+__device__ __forceinline__ void weight_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g,
+                                             int l, int i, int j) {
+    const Lvl v = level(g, l);
+    P.mg_w[v.at(i, j)] = smoother_inv(row_of(P, D, ctot, g, l, v, i, j));
+}
+
+// Level l+1 point (I, J): b = P^T (b_l - A_l x_l), x = W^-1 b.
+__device__ void restrict_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int I,
+                               int J) {
+    const Lvl f = level(g, l), c = level(g, l + 1);
+    const LvlVec vf = vectors(P, l), vc = vectors(P, l + 1);
+    int fx[3], fy[3];
+    double wx[3], wy[3];
+    const int nfx = children(I, g.hx[l], f.m, fx, wx), nfy = children(J, g.hy[l], f.n, fy, wy);
+    double acc = 0.0;
+    for (int b = 0; b < nfy; ++b)
+        for (int a = 0; a < nfx; ++a) {
+            const Row9 r = row_of(P, D, ctot, g, l, f, fx[a], fy[b]);
+            const double res = __ldcg(vf.b + f.at(fx[a], fy[b])) - apply_row(r, vf.x, f, fx[a], fy[b]);
+            acc += wx[a] * wy[b] * res;
+        }
+    const long long at = c.at(I, J);
+    P.mg_b[at] = acc;
+    P.mg_x[at] = winv_at(P, D, ctot, g, l + 1, c, I, J) * acc;
+}
+
+// x_l + P final_{l+1} at (i, j).
+__device__ __forceinline__ double prolonged(const MgDom &g, int l, const Lvl &f, const Lvl &c, const double *x,
+                                            const double *tc, int i, int j) {
+    int px[2], py[2];
+    double ux[2], uy[2];
+    const int npx = parents(i, g.hx[l], c.m, px, ux), npy = parents(j, g.hy[l], c.n, py, uy);
+    double s = __ldcg(x + f.at(i, j));
+    for (int q = 0; q < npy; ++q)
+        for (int p = 0; p < npx; ++p) s += ux[p] * uy[q] * __ldcg(tc + c.at(px[p], py[q]));
+    return s;
+}
+
+// Level l point (i, j): t = x' + W^-1 (b - A x') with x' = x_l + P t_{l+1}.
+__device__ void smooth_up_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int i,
+                                int j) {
+    const Lvl f = level(g, l), c = level(g, l + 1);
+    const LvlVec vf = vectors(P, l);
+    const double *tc = P.mg_t;
+    const Row9 r = row_of(P, D, ctot, g, l, f, i, j);
+    double ax = 0.0, xc = 0.0;
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+            const double a = r.a[dy + 1][dx + 1];
+            if (a == 0.0) continue;
+            const double xp = prolonged(g, l, f, c, vf.x, tc, i + dx, j + dy);
+            ax += a * xp;
+            if (dx == 0 && dy == 0) xc = xp;
+        }
+    const long long at = f.at(i, j);
+    vf.t[at] = xc + winv_at(P, D, ctot, g, l, f, i, j) * (__ldcg(vf.b + at) - ax);
+}
+
+// One Jacobi sweep on level l from `from` into `to`.
+__device__ __forceinline__ void sweep_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g,
+                                            int l, const double *from, double *to, int i, int j) {
+    const Lvl v = level(g, l);
+    const Row9 r = row_of(P, D, ctot, g, l, v, i, j);
+    const long long at = v.at(i, j);
+    const double b = __ldcg(vectors(P, l).b + at);
+    to[at] = __ldcg(from + at) + winv_at(P, D, ctot, g, l, v, i, j) * (b - apply_row(r, from, v, i, j));
+}
+
+// ----------------------------------------------------------- block levels
+// Runs fn(i, j) over every point of level l of the domain with this block.
+template <typename Fn>
+__device__ __forceinline__ void block_points(const MgDom &g, int l, Fn fn) {
+    const int m = g.m[l], tot = m * g.n[l];
+    for (int p = threadIdx.x; p < tot; p += blockDim.x) fn(p % m, p / m);
+}
+
+// The domain's block levels of the set-up: smoother weights of level lc (when
+// lc >= 1; level 0's are formed on the fly), then each coarser operator and
+// its weights.
+__device__ void block_setup(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g) {
+    if (g.lc >= 1) block_points(g, g.lc, [&](int i, int j) { weight_point(P, D, ctot, g, g.lc, i, j); });
+    for (int l = g.lc; l + 1 < g.nlev; ++l) {
+        __syncthreads();
+        block_points(g, l + 1, [&](int i, int j) { galerkin_point(P, D, ctot, g, l, i, j); });
+        __syncthreads();
+        block_points(g, l + 1, [&](int i, int j) { weight_point(P, D, ctot, g, l + 1, i, j); });
+    }
+}
+
+// The domain's block levels of a V-cycle: from x_lc = W^-1 b_lc (already
+// formed) down to the coarsest level, its sweeps, and back up; the result of
+// level lc is left in its t vector.
+__device__ void block_vcycle(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g) {
+    for (int l = g.lc; l + 1 < g.nlev; ++l) {
+        __syncthreads();
+        block_points(g, l + 1, [&](int I, int J) { restrict_point(P, D, ctot, g, l, I, J); });
+    }
+    const int L = g.nlev - 1;
+    const LvlVec vL = vectors(P, L);
+    for (int s = 0; s < MG_COARSE_SWEEPS; ++s) {
+        __syncthreads();
+        const double *from = (s & 1) ? vL.t : vL.x;
+        double *to = (s & 1) ? vL.x : vL.t;
+        block_points(g, L, [&](int i, int j) { sweep_point(P, D, ctot, g, L, from, to, i, j); });
+    }
+    for (int l = L - 1; l >= g.lc; --l) {
+        __syncthreads();
+        block_points(g, l, [&](int i, int j) { smooth_up_point(P, D, ctot, g, l, i, j); });
+    }
+}
+
+// ------------------------------------------------------------ domain sums
+// Sums of the given chunk-partial slots over the domain's level-0 chunks, in
+// chunk order (the same bits in every block).
+template <int NV>
+__device__ __forceinline__ void chunk_sums(const DevPtrs &P, const MgDom &g, const int (&slot)[NV], double (&v)[NV]) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = 0.0;
+    for (int k = threadIdx.x; k < g.c0_count; k += blockDim.x) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] += __ldcg(&P.mg_part[(size_t)slot[i] * P.mg_nchunk0 + g.c0_first + k]);
+    }
+    olf_block_sum<NV>(v);
+}
+
+// The CG's stop decision of a domain after `it` updates of x: converged
+// (||r|| <= tol ||b||), iteration cap, non-finite residual, or a breakdown of
+// the last step (p.q or r.z not positive).
+__device__ __forceinline__ bool mg_stop(const DomainDesc &D, int it, double rr, double bb, double pq, double rz) {
+    const double tol2 = D.overland_tol * D.overland_tol;
+    bool stop = rr <= tol2 * bb || it >= D.overland_maxiter || !(rr == rr);
+    if (it > 0) stop = stop || !(pq > 0.0) || !(rz > 0.0) || !(pq < 1e300);
+    return stop;
+}
+
+struct DomSums {
+    double rr, bb, pq, rz;
+};
+
+__device__ __forceinline__ DomSums decision_sums(const DevPtrs &P, const MgDom &g, int it) {
+    const int slots[4] = {MP_RR, MP_BB, MP_PQ, MP_RZ + ((it + 1) & 1)};  // r.z of iteration it-1
+    double v[4];
+    chunk_sums<4>(P, g, slots, v);
+    return DomSums{v[0], v[1], v[2], v[3]};
+}
+
+}  // namespace
+
+// --------------------------------------------------------------- the solve
+__global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long ctot) {
+    __shared__ double s_sc[2];
+    __shared__ int s_flag;
+    const int tid = threadIdx.x;
+    const int Lg = P.mg_lg;
+    const int nchunk0 = P.mg_nchunk0;
+    double *part = P.mg_part;
+    auto pslot = [&](int slot, int chunk) -> double & { return part[(size_t)slot * nchunk0 + chunk]; };
+    // chunks of level l, block-strided; fn(chunk, MgDom, DomainDesc)
+    auto chunks = [&](int l, auto fn) {
+        for (int k = P.mg_lchunk[l] + blockIdx.x; k < P.mg_lchunk[l + 1]; k += gridDim.x) {
+            const MgChunk ch = P.mgc[k];
+            fn(k, ch, P.mgd[ch.dom], P.dom[ch.dom]);
+        }
+    };
+    auto point_of = [&](const MgChunk &ch, const MgDom &g, int &i, int &j) {
+        const int p = ch.first + tid;
+        if (tid >= ch.count) return false;
+        i = p % g.m[ch.lev];
+        j = p / g.m[ch.lev];
+        return true;
+    };
+    auto active = [&](int d) { return __ldcg(&P.mgctl[d].active) != 0; };
+
+    // ---- S0: r = b - A x, b.b and r.r partials, z = W^-1 r; level-1 operators
+    if (blockIdx.x == 0)
+        for (int d = tid; d < P.ndom; d += blockDim.x) {
+            P.mgctl[d].active = P.mgd[d].nlev > 0 ? 1 : 0;
+            if (P.mgd[d].nlev == 0) {
+                P.octrl[d].iter = 0;
+                P.octrl[d].rr = 0.0;
+                P.octrl[d].bb = 0.0;
+            }
+        }
+    chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+        double v[2] = {0.0, 0.0};
+        int i, j;
+        if (point_of(ch, g, i, j)) {
+            const Lvl f = level(g, 0);
+            const long long c = f.at(i, j);
+            const OlfCoef cf = olf_coef(P, D, c, ctot);
+            const double b = P.olf_b[c];
+            const double r = b - olf_av<false>(cf, P.H, c, f.nx, P.H[c]);
+            P.olf_r[c] = r;
+            P.olf_z[c] = 0.8 / cf.dg * r;
+            v[0] = r * r;
+            v[1] = b * b;
+        }
+        olf_block_sum<2>(v);
+        if (tid == 0) {
+            pslot(MP_RR, k) = v[0];
+            pslot(MP_BB, k) = v[1];
+        }
+    });
+    if (Lg >= 1)
+        chunks(1, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+            int I, J;
+            if (point_of(ch, g, I, J)) galerkin_point(P, D, ctot, g, 0, I, J);
+        });
+    if (!grid_sync(P.barrier)) return;
+    // ---- set-up of the grid levels: A_l and the weights of level l-1
+    for (int l = 2; l <= Lg; ++l) {
+        chunks(l, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+            int I, J;
+            if (point_of(ch, g, I, J)) galerkin_point(P, D, ctot, g, l - 1, I, J);
+        });
+        chunks(l - 1, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+            int i, j;
+            if (ch.lev < g.lc && point_of(ch, g, i, j)) weight_point(P, D, ctot, g, l - 1, i, j);
+        });
+        if (!grid_sync(P.barrier)) return;
+    }
+    // ---- set-up of every domain's block levels
+    for (int d = blockIdx.x; d < P.ndom; d += gridDim.x) {
+        const MgDom &g = P.mgd[d];
+        if (g.nlev > 0) block_setup(P, P.dom[d], ctot, g);
+    }
+    if (!grid_sync(P.barrier)) return;
+
+    // The stop decision after `it` updates of x, taken in the first phase of a
+    // V-cycle by every block for the domains it works on and by block 0 for
+    // all of them (it records the stops and the number of live domains).
+    auto decide_all = [&](int it) {
+        if (blockIdx.x != 0) return;
+        int live = 0;
+        for (int d = 0; d < P.ndom; ++d) {
+            const MgDom &g = P.mgd[d];
+            if (!active(d)) continue;
+            const DomSums s = decision_sums(P, g, it);
+            if (mg_stop(P.dom[d], it, s.rr, s.bb, s.pq, s.rz)) {
+                if (tid == 0) {
+                    P.mgctl[d].active = 0;
+                    P.octrl[d].iter = it;
+                    P.octrl[d].rr = s.rr;
+                    P.octrl[d].bb = s.bb;
+                }
+            } else {
+                ++live;
+            }
+        }
+        if (tid == 0) P.gctrl->olf_live[0] = live;
+    };
+    // (block 0 may clear a domain's flag during this phase, so one thread reads
+    // it for the whole block: the block then takes one path)
+    auto live_after = [&](int d, int it, int &cache_dom, bool &cache_live) {
+        if (d != cache_dom) {
+            cache_dom = d;
+            if (tid == 0) s_flag = active(d) ? 1 : 0;
+            __syncthreads();
+            cache_live = s_flag != 0;
+            __syncthreads();
+            if (cache_live) {
+                const DomSums s = decision_sums(P, P.mgd[d], it);
+                cache_live = !mg_stop(P.dom[d], it, s.rr, s.bb, s.pq, s.rz);
+            }
+        }
+        return cache_live;
+    };
+
+    for (int it = 0;; ++it) {
+        // ---- down: restriction with the residual fused, grid levels
+        for (int l = 0; l < Lg; ++l) {
+            if (l == 0) decide_all(it);
+            int cd = -1;
+            bool cl = false;
+            chunks(l + 1, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+                const bool go = l == 0 ? live_after(ch.dom, it, cd, cl) : active(ch.dom);
+                int I, J;
+                if (go && point_of(ch, g, I, J)) restrict_point(P, D, ctot, g, l, I, J);
+            });
+            if (!grid_sync(P.barrier)) return;
+            if (l == 0 && __ldcg(&P.gctrl->olf_live[0]) == 0) return;
+        }
+        // ---- the domains' block levels
+        if (Lg == 0) decide_all(it);
+        {
+            int cd = -1;
+            bool cl = false;
+            for (int d = blockIdx.x; d < P.ndom; d += gridDim.x) {
+                const MgDom &g = P.mgd[d];
+                const bool go = Lg == 0 ? live_after(d, it, cd, cl) : active(d);
+                if (go && g.nlev > 0) block_vcycle(P, P.dom[d], ctot, g);
+            }
+        }
+        if (!grid_sync(P.barrier)) return;
+        if (Lg == 0 && __ldcg(&P.gctrl->olf_live[0]) == 0) return;
+        // ---- up: prolongation with the post-smoothing fused, grid levels
+        for (int l = Lg - 1; l >= 1; --l) {
+            chunks(l, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+                int i, j;
+                if (ch.lev < g.lc && active(ch.dom) && point_of(ch, g, i, j)) smooth_up_point(P, D, ctot, g, l, i, j);
+            });
+            if (!grid_sync(P.barrier)) return;
+        }
+        // ---- level 0: z (the preconditioned residual, in olf_w) and r.z
+        chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+            if (!active(ch.dom)) return;
+            double v[1] = {0.0};
+            int i, j;
+            if (point_of(ch, g, i, j)) {
+                if (g.lc > 0) smooth_up_point(P, D, ctot, g, 0, i, j);
+                const long long c = level(g, 0).at(i, j);
+                v[0] = __ldcg(P.olf_r + c) * __ldcg(P.olf_w + c);
+            }
+            olf_block_sum<1>(v);
+            if (tid == 0) pslot(MP_RZ + (it & 1), k) = v[0];
+        });
+        if (!grid_sync(P.barrier)) return;
+        // ---- X: p = z + beta p, q = A z + beta q, p.q
+        {
+            int cd = -1;
+            chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+                if (!active(ch.dom)) return;
+                if (ch.dom != cd) {
+                    cd = ch.dom;
+                    const int slots[2] = {MP_RZ + (it & 1), MP_RZ + ((it + 1) & 1)};
+                    double v[2];
+                    chunk_sums<2>(P, g, slots, v);
+                    if (tid == 0) s_sc[0] = it == 0 ? 0.0 : v[0] / v[1];
+                    __syncthreads();
+                }
+                const double beta = s_sc[0];
+                double pq[1] = {0.0};
+                int i, j;
+                if (point_of(ch, g, i, j)) {
+                    const Lvl f = level(g, 0);
+                    const long long c = f.at(i, j);
+                    const OlfCoef cf = olf_coef(P, D, c, ctot);
+                    const double z = __ldcg(P.olf_w + c);
+                    const double az = olf_av<true>(cf, P.olf_w, c, f.nx, z);
+                    const double p = it == 0 ? z : z + beta * P.olf_p[c];
+                    const double q = it == 0 ? az : az + beta * P.olf_s[c];
+                    P.olf_p[c] = p;
+                    P.olf_s[c] = q;
+                    pq[0] = p * q;
+                }
+                olf_block_sum<1>(pq);
+                if (tid == 0) pslot(MP_PQ, k) = pq[0];
+            });
+        }
+        if (!grid_sync(P.barrier)) return;
+        // ---- Y: x += alpha p, r -= alpha q, r.r, z = W^-1 r
+        {
+            int cd = -1;
+            chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+                if (!active(ch.dom)) return;
+                if (ch.dom != cd) {
+                    cd = ch.dom;
+                    const int slots[2] = {MP_RZ + (it & 1), MP_PQ};
+                    double v[2];
+                    chunk_sums<2>(P, g, slots, v);
+                    if (tid == 0) s_sc[1] = (v[1] > 0.0 && v[0] > 0.0 && v[1] < 1e300) ? v[0] / v[1] : 0.0;
+                    __syncthreads();
+                }
+                const double alpha = s_sc[1];
+                double rr[1] = {0.0};
+                int i, j;
+                if (point_of(ch, g, i, j)) {
+                    const long long c = level(g, 0).at(i, j);
+                    const OlfCoef cf = olf_coef(P, D, c, ctot);
+                    P.H[c] += alpha * P.olf_p[c];
+                    const double r = P.olf_r[c] - alpha * P.olf_s[c];
+                    P.olf_r[c] = r;
+                    P.olf_z[c] = 0.8 / cf.dg * r;
+                    rr[0] = r * r;
+                }
+                olf_block_sum<1>(rr);
+                if (tid == 0) pslot(MP_RR, k) = rr[0];
+            });
+        }
+        if (!grid_sync(P.barrier)) return;
+    }
+}
+
+// ------------------------------------------------------------------- host
+void mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::vector<MgChunk> &chunks,
+             int (&lchunk)[MG_MAXLEV + 2], int &lg, long long &nc) {
+    const int nd = (int)doms.size();
+    mgd.assign(nd, MgDom{});
+    nc = 0;
+    lg = 0;
+    for (int d = 0; d < nd; ++d) {
+        const DomainDesc &D = doms[d];
+        MgDom &g = mgd[d];
+        std::memset(&g, 0, sizeof(g));
+        g.nx = D.nx;
+        g.off[0] = D.off2;
+        int m = D.nx - 2, n = D.ny - 2;
+        if (m < 1 || n < 1) continue;  // no interior cell: nothing to solve
+        int L = 0;
+        g.m[0] = m;
+        g.n[0] = n;
+        while ((m >= 3 || n >= 3) && L + 1 < MG_MAXLEV) {
+            g.hx[L] = m >= 3;
+            g.hy[L] = n >= 3;
+            m = g.hx[L] ? m / 2 : m;
+            n = g.hy[L] ? n / 2 : n;
+            ++L;
+            g.m[L] = m;
+            g.n[L] = n;
+            g.off[L] = nc;
+            nc += (long long)m * n;
+        }
+        g.nlev = L + 1;
+        g.lc = 0;
+        while (g.lc < g.nlev - 1 && (long long)g.m[g.lc] * g.n[g.lc] > MG_BLOCK_PTS) ++g.lc;
+        lg = std::max(lg, g.lc);
+    }
+    // chunk lists: level 0 for every domain with an interior (the CG's
+    // vectors), level l >= 1 for the domains whose grid phases write it
+    chunks.clear();
+    for (int l = 0; l <= MG_MAXLEV; ++l) {
+        lchunk[l] = (int)chunks.size();
+        if (l > lg) continue;
+        for (int d = 0; d < nd; ++d) {
+            MgDom &g = mgd[d];
+            if (g.nlev == 0 || (l > 0 && l > g.lc)) continue;
+            const int tot = g.m[l] * g.n[l];
+            if (l == 0) g.c0_first = (int)chunks.size();
+            for (int f = 0; f < tot; f += OLF_THREADS)
+                chunks.push_back(MgChunk{d, l, f, std::min(OLF_THREADS, tot - f)});
+            if (l == 0) g.c0_count = (int)chunks.size() - g.c0_first;
+        }
+    }
+    lchunk[MG_MAXLEV + 1] = (int)chunks.size();
+}
+
+cudaError_t configure_mg(LaunchCfg &L, int device) {
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_mgcg, OLF_THREADS, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    L.mg_blocks = per_sm * prop.multiProcessorCount;
+    return cudaSuccess;
+}
+
+cudaError_t launch_overland_mg(const DevPtrs &P, const LaunchCfg &L, long long ctot, cudaStream_t s) {
+    DevPtrs args = P;
+    long long c = ctot;
+    void *kargs[] = {&args, &c};
+    int need = P.ndom;
+    for (int l = 0; l <= P.mg_lg; ++l) need = std::max(need, P.mg_lchunk[l + 1] - P.mg_lchunk[l]);
+    const int grid = std::max(1, std::min(L.mg_blocks, need));
+    return cudaLaunchCooperativeKernel((const void *)k_olf_mgcg, dim3(grid), dim3(OLF_THREADS), kargs, 0, s);
+}

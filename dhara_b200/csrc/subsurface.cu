@@ -571,6 +571,33 @@ __device__ __forceinline__ Masks masks_of(const ColumnRef &cr) {
     return m;
 }
 
+// Face weights of a column for the T operator: the stencil weight times the
+// 1/2 of the face average, zero on a domain face, so that a face coefficient
+// is one add and one multiply, f = h (K_c + K_nb).  The vertical coefficient
+// of the face between planes k and k+1 is the same number seen from either
+// cell (IEEE addition commutes), so it is computed once and carried.
+template <typename T>
+struct FaceW {
+    T w, e, s, n, z;
+};
+template <typename T>
+__device__ __forceinline__ FaceW<T> face_weights(const ColumnRef &cr, const StencilW<T> &w) {
+    FaceW<T> f;
+    f.w = cr.i > 0 ? T(0.5) * w.cx : T(0);
+    f.e = cr.i < cr.nx - 1 ? T(0.5) * w.cx : T(0);
+    f.s = cr.j > 0 ? T(0.5) * w.cy : T(0);
+    f.n = cr.j < cr.ny - 1 ? T(0.5) * w.cy : T(0);
+    f.z = T(0.5) * w.cz;
+    return f;
+}
+
+// Diagonal of the column block of M without its vertical couplings (the same
+// expression in the factorisation and in the inner sweep's M z).
+template <typename T>
+__device__ __forceinline__ T lateral_diag(T Dk, T fw, T fe, T fs, T fn) {
+    return (Dk + (fw + fe)) + (fs + fn);
+}
+
 // Chunk issue of each phase for tile `tile` (thread 0 only): arms buffer b's
 // mbarrier with the chunk's bytes and starts one TMA box load per array.
 template <typename T>
@@ -658,9 +685,11 @@ __device__ __forceinline__ void phase_R(const DevPtrs &P, int tile, int tile_nex
     };
     const int nz = cr.nz, hc = H.hc, oc = threadIdx.x;
     const Masks M = masks_of(cr);
+    const FaceW<T> f = face_weights(cr, w);
     const double cx = (double)w.cx, cy = (double)w.cy, cz = (double)w.cz;
     double x_up = 0.0, K_up = 0.0;
-    T cprev = T(0), yprev = T(0);
+    T cprev = T(0), yprev = T(0), fd = T(0);
+    T a2 = T(0);  // r.M^-1 r of the column, summed in T
     auto plane = [&](int b, int pl, int k) {
         if (!cr.valid) return;
         const double *sx = (const double *)buf(b) + pl * H.plane;
@@ -690,27 +719,30 @@ __device__ __forceinline__ void phase_R(const DevPtrs &P, int tile, int tile_nex
         v[1] += bk * bk;
         const T rT = (T)rk;
         const long long g = cr.g0 + (long long)k * cr.sxy;
+        // the column block of M from the T coefficients: diagonal bl + fd + fu,
+        // sub-diagonal -fd, super-diagonal -fu
         const T Kt = (T)Kc;
-        const T kdT = T(mu) * (T(0.5) * (Kt + (T)K_up)), kuT = T(md) * (T(0.5) * (Kt + (T)K_dn));
-        const T kwT = T(M.w) * (T(0.5) * (Kt + (T)Kw)), keT = T(M.e) * (T(0.5) * (Kt + (T)Ke));
-        const T ksT = T(M.s) * (T(0.5) * (Kt + (T)Ks)), knT = T(M.n) * (T(0.5) * (Kt + (T)Kn));
-        const T bd = (T)Dk + w.cx * (kwT + keT) + w.cy * (ksT + knT) + w.cz * (kdT + kuT);
-        const T a = -w.cz * kdT, c = -w.cz * kuT;
-        const T den = bd - a * cprev;
+        const T fw = f.w * (Kt + (T)Kw), fe = f.e * (Kt + (T)Ke);
+        const T fs = f.s * (Kt + (T)Ks), fn = f.n * (Kt + (T)Kn);
+        const T fu = k + 1 < nz ? f.z * (Kt + (T)K_dn) : T(0);
+        const T bd = (lateral_diag((T)Dk, fw, fe, fs, fn) + fd) + fu;
+        const T den = bd + fd * cprev;  // b_k - a_k c'_{k-1} with a_k = -fd
         const T inv = fixed ? T(0) : recip(den);
-        const T cp = c * inv;
+        const T cp = -fu * inv;
         const T y = rT - cprev * yprev;
         const T dp = y * inv;
         finv[g] = inv;
         fc[g] = cp;
         put_dprime<T, DSMEM>(dp, s_d, k, z + g);
-        v[2] += (double)y * (double)dp;
+        a2 += y * dp;
         cprev = cp;
         yprev = y;
+        fd = fu;
         x_up = xc;
         K_up = Kc;
     };
     march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next);
+    v[2] = (double)a2;
     if (cr.valid) back_sweep<T, DSMEM>(cr, s_d, fc, z);
 }
 
@@ -721,7 +753,16 @@ __device__ __forceinline__ void phase_R(const DevPtrs &P, int tile, int tile_nex
 // lateral neighbours (from the staged halo boxes) and at k+1; q = A p;
 // t = M^-1 q by the stored factors (forward sweep in the march, back sweep
 // after it); d += ap p_prev.  Writes z, p, t into the buffers other than
-// `prev`, and v = {p.q, z.q, q.t, z.M z}.
+// `prev`, and v = {p.q, z.q, q.t, z.M z} (each column's sums taken in T).
+// The values at k+1 (z, p, K and the vertical face coefficient) are carried
+// to the next plane as its own.  The three forms of a sweep (a cycle's first
+// without or with the previous direction, and the general one) are compiled
+// separately: MODE 0 p = z, 1 p = z + bt p_prev, 2 z and p from t and p_prev.
+template <int M_>
+struct SweepMode {
+    static constexpr int value = M_;
+};
+
 template <typename T, bool DSMEM, int TXC>
 __device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_next, bool prefetched, bool first_next,
                         bool keep_next, int prev_next, const ColumnRef &cr, const StencilW<T> &w, T ap, T bt,
@@ -747,70 +788,93 @@ __device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_nex
             });
     };
     const int nz = cr.nz, hc = H.hc, oc = threadIdx.x;
-    const Masks M = masks_of(cr);
-    const T mW = (T)M.w, mE = (T)M.e, mS = (T)M.s, mN = (T)M.n;
-    T p_up = T(0), z_up = T(0), K_up = T(0), cprev = T(0), yprev = T(0);
-    // this iteration's z and p at offset o of staged halo planes (z, t, p)
-    auto zv = [&](const T *zz, const T *tt, int o) { return first ? zz[o] : zz[o] - ap * tt[o]; };
-    auto pv = [&](const T *zz, const T *tt, const T *pp, int o) {
-        return first ? (keep_p ? zz[o] + bt * pp[o] : zz[o]) : (zz[o] - ap * tt[o]) + bt * pp[o];
-    };
-    auto plane = [&](int b, int pl, int k) {
-        if (!cr.valid) return;
-        const T *sz = (const T *)buf(b) + pl * H.plane;
-        const T *st = (const T *)(buf(b) + HB) + pl * H.plane;
-        const T *sp = (const T *)(buf(b) + 2 * HB) + pl * H.plane;
-        const T *sK = (const T *)(buf(b) + 3 * HB) + pl * H.plane;
-        const T *own = (const T *)(buf(b) + 4 * HB) + pl * OWN_PLANE + oc;
-        const T Dk = own[0], inv = own[S], cp = own[2 * S];
-        const T zc = zv(sz, st, hc), pc = pv(sz, st, sp, hc);
-        T z_dn = T(0), p_dn = T(0), K_dn = T(0);
-        if (k + 1 < nz) {
-            if (pl + 1 < CHN) {
-                z_dn = zv(sz + H.plane, st + H.plane, hc);
-                p_dn = pv(sz + H.plane, st + H.plane, sp + H.plane, hc);
-                K_dn = sK[H.plane + hc];
-            } else {
-                const unsigned char *nb = buf((b + 1) % STAGES);
-                const T *nzz = (const T *)nb, *ntt = (const T *)(nb + HB), *npp = (const T *)(nb + 2 * HB);
-                z_dn = zv(nzz, ntt, hc);
-                p_dn = pv(nzz, ntt, npp, hc);
-                K_dn = ((const T *)(nb + 3 * HB))[hc];
+    const FaceW<T> f = face_weights(cr, w);
+    // carried down the column: this plane's z, p, K and upper face coefficient,
+    // the plane above's z and p, the forward sweep's c'_{k-1} and y_{k-1}
+    T zc = T(0), pc = T(0), Kc = T(0), fd = T(0), z_up = T(0), p_up = T(0), cprev = T(0), yprev = T(0);
+    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+    long long g = cr.g0;
+    auto sweep = [&](auto mode) {
+        constexpr int MODE = decltype(mode)::value;
+        auto zv = [&](const T *zz, const T *tt, int o) {
+            if constexpr (MODE == 2) return zz[o] - ap * tt[o];
+            else return zz[o];
+        };
+        auto pz = [&](T z, const T *pp, int o) {  // p from this iteration's z
+            if constexpr (MODE == 0) return z;
+            else return z + bt * pp[o];
+        };
+        auto plane = [&](int b, int pl, int k) {
+            if (!cr.valid) return;
+            const T *sz = (const T *)buf(b) + pl * H.plane;
+            const T *st = (const T *)(buf(b) + HB) + pl * H.plane;
+            const T *sp = (const T *)(buf(b) + 2 * HB) + pl * H.plane;
+            const T *sK = (const T *)(buf(b) + 3 * HB) + pl * H.plane;
+            const T *own = (const T *)(buf(b) + 4 * HB) + pl * OWN_PLANE + oc;
+            if (k == 0) {
+                zc = zv(sz, st, hc);
+                pc = pz(zc, sp, hc);
+                Kc = sK[hc];
             }
-        }
-        const T Kc = sK[hc];
-        const T mu = k > 0 ? T(1) : T(0), md = k < nz - 1 ? T(1) : T(0);
-        const T kd = mu * (T(0.5) * (Kc + K_up)), ku = md * (T(0.5) * (Kc + K_dn));
-        const T kw = mW * (T(0.5) * (Kc + sK[hc - 1])), ke = mE * (T(0.5) * (Kc + sK[hc + 1]));
-        const T ks = mS * (T(0.5) * (Kc + sK[hc - H.bw])), kn = mN * (T(0.5) * (Kc + sK[hc + H.bw]));
-        const bool fixed = Dk < T(0);  // Dirichlet cell: identity row, z = p = 0 there
-        T q = Dk * pc + w.cx * (kw * (pc - pv(sz, st, sp, hc - 1)) + ke * (pc - pv(sz, st, sp, hc + 1))) +
-              w.cy * (ks * (pc - pv(sz, st, sp, hc - H.bw)) + kn * (pc - pv(sz, st, sp, hc + H.bw))) +
-              w.cz * (kd * (pc - p_up) + ku * (pc - p_dn));
-        // (M z)_k with M the column's tridiagonal part of A
-        T Mz = (Dk + w.cx * (kw + ke) + w.cy * (ks + kn)) * zc + w.cz * (kd * (zc - z_up) + ku * (zc - z_dn));
-        if (fixed) {
-            q = T(0);
-            Mz = T(0);
-        }
-        v[0] += (double)pc * (double)q;
-        v[1] += (double)zc * (double)q;
-        v[3] += (double)zc * (double)Mz;
-        const T y = q - cprev * yprev;
-        const T dp = y * inv;
-        v[2] += (double)y * (double)dp;
-        const long long g = cr.g0 + (long long)k * cr.sxy;
-        z_out[g] = zc;
-        p_out[g] = pc;
-        d[g] = first ? T(0) : own[3 * S] + ap * sp[hc];
-        put_dprime<T, DSMEM>(dp, s_d, k, t_out + g);
-        cprev = cp;
-        yprev = y;
-        p_up = pc;
-        z_up = zc;
-        K_up = Kc;
+            const T Dk = own[0], inv = own[S], cp = own[2 * S];
+            T z_dn = T(0), p_dn = T(0), K_dn = T(0), fu = T(0);
+            if (k + 1 < nz) {
+                const T *nzz = sz + H.plane, *ntt = st + H.plane, *npp = sp + H.plane, *nK = sK + H.plane;
+                if (pl + 1 == CHN) {
+                    const unsigned char *nb = buf((b + 1) % STAGES);
+                    nzz = (const T *)nb;
+                    ntt = (const T *)(nb + HB);
+                    npp = (const T *)(nb + 2 * HB);
+                    nK = (const T *)(nb + 3 * HB);
+                }
+                z_dn = zv(nzz, ntt, hc);
+                p_dn = pz(z_dn, npp, hc);
+                K_dn = nK[hc];
+                fu = f.z * (Kc + K_dn);
+            }
+            const T fw = f.w * (Kc + sK[hc - 1]), fe = f.e * (Kc + sK[hc + 1]);
+            const T fs = f.s * (Kc + sK[hc - H.bw]), fn = f.n * (Kc + sK[hc + H.bw]);
+            const T pw = pz(zv(sz, st, hc - 1), sp, hc - 1), pe = pz(zv(sz, st, hc + 1), sp, hc + 1);
+            const T ps = pz(zv(sz, st, hc - H.bw), sp, hc - H.bw), pn = pz(zv(sz, st, hc + H.bw), sp, hc + H.bw);
+            const bool fixed = Dk < T(0);  // Dirichlet cell: identity row, z = p = 0 there
+            T q = Dk * pc + (fw * (pc - pw) + fe * (pc - pe)) + (fs * (pc - ps) + fn * (pc - pn)) +
+                  (fd * (pc - p_up) + fu * (pc - p_dn));
+            // (M z)_k with M the column's tridiagonal part of A
+            T Mz = lateral_diag(Dk, fw, fe, fs, fn) * zc + (fd * (zc - z_up) + fu * (zc - z_dn));
+            if (fixed) {
+                q = T(0);
+                Mz = T(0);
+            }
+            a0 += pc * q;
+            a1 += zc * q;
+            a3 += zc * Mz;
+            const T y = q - cprev * yprev;
+            const T dp = y * inv;
+            a2 += y * dp;
+            z_out[g] = zc;
+            p_out[g] = pc;
+            if constexpr (MODE == 2) d[g] = own[3 * S] + ap * sp[hc];
+            else d[g] = T(0);
+            put_dprime<T, DSMEM>(dp, s_d, k, t_out + g);
+            cprev = cp;
+            yprev = y;
+            p_up = pc;
+            z_up = zc;
+            zc = z_dn;
+            pc = p_dn;
+            Kc = K_dn;
+            fd = fu;
+            g += cr.sxy;
+        };
+        march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next);
     };
-    march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next);
+    if (!first) sweep(SweepMode<2>{});
+    else if (keep_p) sweep(SweepMode<1>{});
+    else sweep(SweepMode<0>{});
+    v[0] = (double)a0;
+    v[1] = (double)a1;
+    v[2] = (double)a2;
+    v[3] = (double)a3;
     if (cr.valid) back_sweep<T, DSMEM>(cr, s_d, fc, t_out);
 }
 
@@ -1202,34 +1266,48 @@ __global__ void __launch_bounds__(TILE_THREADS) k_epilogue(DevPtrs P) {
 // krylov_solve) in the same order, so the results are those of the
 // launch-per-kernel sequence bit for bit; the loop ends as soon as every
 // domain's Picard iteration is done.
+// The phases other than the solve are called, not inlined, so that each gets
+// its own register allocation under the kernel's limit and the solve loop
+// keeps the registers it has in k_krylov.
+enum StepPhase { PH_PROLOGUE, PH_ASSEMBLE, PH_DIR_FIXED, PH_DIR_ROWS, PH_CHECK, PH_EPILOGUE };
+
+template <typename T, int PH>
+__device__ __noinline__ void step_phase(const DevPtrs &P) {
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        if constexpr (PH == PH_PROLOGUE) prologue_tile(P, t);
+        else if constexpr (PH == PH_ASSEMBLE) assemble_tile<T>(P, t);
+        else if constexpr (PH == PH_DIR_FIXED) dir_fixed_tile<T>(P, t);
+        else if constexpr (PH == PH_DIR_ROWS) dir_rows_tile<T>(P, t);
+        else if constexpr (PH == PH_CHECK) picard_check_tile(P, t);
+        else epilogue_tile<T>(P, t);
+    }
+}
+
 template <typename T, int TXC>
 __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 4 ? KRYLOV_BLOCKS_F32 : KRYLOV_BLOCKS_F64)
-    k_step(DevPtrs P, int maxiter, int dirichlet) {
+    k_step(const __grid_constant__ DevPtrs P, int maxiter, int dirichlet) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar[STAGES];
     constexpr bool DSMEM = sizeof(T) == 4 && KRYLOV_DSMEM_F32;
     const SolveSmem<T> sm = solve_smem<T, DSMEM>(P, smem_raw, s_bar);
     StageBars sb{s_bar, 0u, P.barrier, 0u};
-    auto tiles = [&](auto fn) {
-        for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) fn(t);
-    };
-    tiles([&](int t) { prologue_tile(P, t); });
+    step_phase<T, PH_PROLOGUE>(P);
     if (!grid_sync(P.barrier)) return;
     for (int m = 0; m < maxiter; ++m) {
-        tiles([&](int t) { assemble_tile<T>(P, t); });
+        step_phase<T, PH_ASSEMBLE>(P);
         if (!grid_sync(P.barrier)) return;
         if (dirichlet) {
-            tiles([&](int t) { dir_fixed_tile<T>(P, t); });
+            step_phase<T, PH_DIR_FIXED>(P);
             if (!grid_sync(P.barrier)) return;
-            tiles([&](int t) { dir_rows_tile<T>(P, t); });
+            step_phase<T, PH_DIR_ROWS>(P);
             if (!grid_sync(P.barrier)) return;
         }
         if (!krylov_solve<T, DSMEM, TXC>(P, sm, sb)) return;
-        tiles([&](int t) { picard_check_tile(P, t); });
+        step_phase<T, PH_CHECK>(P);
         if (!grid_sync(P.barrier)) return;
         if (ldcg(&P.gctrl->n_picard) == 0) break;
     }
-    tiles([&](int t) { epilogue_tile<T>(P, t); });
+    step_phase<T, PH_EPILOGUE>(P);
 }
 
 // Evaluates the closure at psi^n into out: which = 0 theta, 1 K, 2 C.
@@ -1365,6 +1443,9 @@ cudaError_t configure_3d(LaunchCfg &L, int device, int ntiles) {
     L.krylov_per_sm = per_sm;
     L.step_per_sm = step_sm < per_sm ? step_sm : per_sm;
     if (L.step_per_sm < 1) return cudaErrorInvalidConfiguration;
+    // one launch per subsurface step by default, where the fused kernel keeps
+    // the Krylov kernel's occupancy
+    L.fused_step = L.step_per_sm >= L.krylov_per_sm ? 1 : 0;
     (void)ntiles;
     return cudaSuccess;
 }

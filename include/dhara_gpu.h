@@ -114,7 +114,15 @@ typedef struct {
      * atomic.  Saturation is not a switch of the loss (theta and K are
      * continuous there) but of the closure's formula. */
     int32_t record_branches;
-    int32_t reserved_i[5];
+    /* Overland linear solver (the same system and stopping rule either way):
+     * 0 (the default) conjugate gradients preconditioned by a geometric
+     * multigrid V-cycle (Galerkin coarse operators, weighted-Jacobi
+     * smoothing), which converges in tens of iterations where ponded cells
+     * make the system stiff; 1 pipelined point-Jacobi-preconditioned CG (one
+     * grid barrier per iteration, thousands of iterations on stiff systems).
+     * Every domain of a handle uses the same solver. */
+    int32_t overland_solver;
+    int32_t reserved_i[4];
     double reserved_d[8];
 } dhara_params;
 
@@ -295,8 +303,10 @@ typedef struct {
     double krylov_ms;     /* per trial step of the chosen schedule (autotune only) */
     double overland_ms;
     /* 1: each subsurface step is one persistent launch (prologue, every Picard
-     * iteration's assembly, solve and check, epilogue); 0: a launch per kernel
-     * (the default; per-kernel timing then names every phase) */
+     * iteration's assembly, solve and check, epilogue) -- the default where
+     * that kernel runs as many blocks per SM as the Krylov kernel; 0: a launch
+     * per kernel (per-kernel timing then names every phase).  Results are the
+     * same bit for bit. */
     int32_t fused_step;
     int32_t pad;
 } dhara_launch_config;

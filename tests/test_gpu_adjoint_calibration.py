@@ -15,11 +15,12 @@ iterations every step) over a shortened horizon of 10 steps:
   accepted only for a step h whose +h and -h runs took exactly the branches
   of the unperturbed run (dhara_diagnostics' branch_signature over those
   decisions and the Picard counts); accepted differences agree to 1e-4
-  relative where the gradient is significant, and to 1e-6 of the largest
-  gradient elsewhere.  The difference runs solve to 1e-13 (3D) and 1e-12
-  (overland, up to 50,000 iterations), so that the loss's noise stays below
-  those bounds; the overland iteration counts are part of the branch pattern
-  (a CG that stops at another iteration is another map).
+  relative where the gradient is significant, and elsewhere to 1e-6 of the
+  largest gradient plus the loss's noise over 2h.  The difference runs solve
+  to 1e-13 (3D) and 1e-12 (overland, up to 50,000 iterations), so the loss
+  is known to about 1e-13 of itself and a difference to 1e-13 |L| / h; the
+  overland iteration counts are part of the branch pattern (a CG that stops
+  at another iteration is another map).
 
 The forward this reverses is src/subsurface.cu:686-847 + src/overland.cu:387-419.
 """
@@ -161,6 +162,7 @@ def test_calibration_gradient_matches_central_differences(gpu, tight):
     report = {}
     for field, g, ncells in (("ksat", g_lk, 32), ("alpha", g_al, 8), ("nvg", g_n, 8)):
         scale = float(np.max(np.abs(g)))
+        noise = 1e-13 * abs(L)  # half the spread of the loss between two runs of one map
         cells = rng.choice(N, ncells, replace=False)
         accepted = worst = 0.0
         for c in cells:
@@ -173,11 +175,11 @@ def test_calibration_gradient_matches_central_differences(gpu, tight):
                 assert err <= 1e-4, (field, int(c), h, g[c], fd)
             else:
                 err = abs(g[c] - fd) / scale
-                assert err <= 1e-6, (field, int(c), h, g[c], fd)
+                assert abs(g[c] - fd) <= 1e-6 * scale + noise / h, (field, int(c), h, g[c], fd, L)
             worst = max(worst, err)
         report[field] = (int(accepted), len(cells), worst)
         assert accepted >= len(cells) // 2, (field, accepted)
-    print("cells accepted / drawn / worst error:", report)
+    print("loss", L, "cells accepted / drawn / worst error:", report)
 
 
 def test_calibration_taylor_direction(gpu, tight):
