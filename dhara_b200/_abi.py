@@ -48,7 +48,8 @@ class Params(ct.Structure):
         ("krylov_maxiter", ct.c_int32), ("theta_update", ct.c_int32), ("krylov_tol", ct.c_double),
         ("overland_maxiter", ct.c_int32), ("precision", ct.c_int32), ("overland_tol", ct.c_double),
         ("inner_tol", ct.c_double), ("inner_maxiter", ct.c_int32), ("closure_fp32", ct.c_int32),
-        ("record_branches", ct.c_int32), ("overland_solver", ct.c_int32), ("reserved_i", ct.c_int32 * 4), ("reserved_d", ct.c_double * 8),
+        ("record_branches", ct.c_int32), ("overland_solver", ct.c_int32), ("dt_halvings", ct.c_int32),
+        ("reserved_i", ct.c_int32 * 3), ("reserved_d", ct.c_double * 8),
     ]
 
 
@@ -65,7 +66,8 @@ class Diagnostics(ct.Structure):
         ("bottom_outflow_cum", ct.c_double), ("rain_cum", ct.c_double),
         ("overland_boundary_out_cum", ct.c_double), ("overland_clip_cum", ct.c_double),
         ("ponded_volume", ct.c_double), ("picard_err_last", ct.c_double),
-        ("krylov_relres_last", ct.c_double), ("branch_signature", ct.c_uint64), ("reserved", ct.c_double * 5),
+        ("krylov_relres_last", ct.c_double), ("branch_signature", ct.c_uint64),
+        ("substeps_total", ct.c_int64), ("step_attempts_total", ct.c_int64), ("reserved", ct.c_double * 3),
     ]
 
     def as_dict(self):

@@ -68,6 +68,12 @@ struct dhara_handle {
     std::vector<std::vector<double>> sched;
     std::vector<unsigned> uploaded;  // bitmask per domain
     bool prepared = false;
+    // time-step halving (dt_halvings): the saved step state, per-domain
+    // actions, and the accepted / attempted step counts per domain
+    int max_halvings = 0;
+    StepState substate{};
+    int *d_action = nullptr;
+    std::vector<long long> substeps, attempts;
     // graph replay
     cudaGraphExec_t graph_exec = nullptr;
     bool graph_failed = false;
@@ -143,6 +149,8 @@ int validate(const dhara_params &p, int d) {
         return fail(DHARA_ERR_INVALID, "domain %d: tolerances must be > 0", d);
     if (p.overland_solver < 0 || p.overland_solver > 1)
         return fail(DHARA_ERR_INVALID, "domain %d: unknown overland_solver %d", d, p.overland_solver);
+    if (p.dt_halvings < 0 || p.dt_halvings > 20)
+        return fail(DHARA_ERR_INVALID, "domain %d: dt_halvings must be in [0, 20]", d);
     return DHARA_OK;
 }
 
@@ -650,6 +658,9 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         D.closure_fp32 = (h->mixed && p.closure_fp32) ? 1 : 0;
         D.closure_fast = (h->mixed && !p.closure_fp32) ? 1 : 0;
         D.record_branches = p.record_branches & 127;
+        D.sub_frac = 1.0;
+        D.step_advance = 1;
+        h->max_halvings = std::max(h->max_halvings, (int)p.dt_halvings);
         // overland segments: runs of up to OLF_SEG surface cells of this domain
         {
             const int first = (int)h->hsegs.size();
@@ -823,6 +834,18 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         if (rc2) return bail(rc2);
     }
 
+    h->substeps.assign(ndomains, 0);
+    h->attempts.assign(ndomains, 0);
+    if (h->max_halvings > 0) {
+        StepState &S = h->substate;
+        rc |= dalloc(h, &S.psin, N);
+        rc |= dalloc(h, &S.thetan, N);
+        for (double **q : {&S.ktop, &S.ph, &S.h, &S.H}) rc |= dalloc(h, q, C);
+        rc |= dalloc(h, &S.diag, ndomains);
+        rc |= dalloc(h, &h->d_action, ndomains);
+        if (rc) return bail(DHARA_ERR_NOMEM);
+        S.action = h->d_action;
+    }
     h->L.nz_max = h->nz_max;
     h->L.mixed = h->mixed;
     h->L.olf_mg = params[0].overland_solver == 0 ? 1 : 0;
@@ -1122,11 +1145,99 @@ int dhara_overland_step(dhara_handle *h) {
     return enqueue_overland(h);
 }
 
+namespace {
+
+// Steps with time-step halving: every round of attempts advances each domain
+// that still has time left in the step by its current sub-step, dt / 2^k.  A
+// domain whose Picard iteration converged (or that is at its smallest
+// sub-step) keeps the result and saves it; one that did not is restored to
+// its last saved state and halves.  A domain that has finished the step is
+// frozen for the further rounds (no Picard iteration, no overland solve with
+// the multigrid solver) and restored after each.  The host reads the Picard
+// outcome once per round.
+int step_halving(dhara_handle *h, int nsteps) {
+    const DevPtrs &P = h->P;
+    cudaStream_t s = h->stream;
+    if (h->stats_steps > 0) return fail(DHARA_ERR_UNSUPPORTED, "layer statistics are not kept with dt_halvings");
+    const int nd = h->ndom, K = h->max_halvings;
+    std::vector<int> act(nd), k(nd);
+    std::vector<long long> rem(nd);
+    std::vector<PicardCtrl> pc(nd);
+    auto run_actions = [&]() -> int {
+        CK(cudaMemcpyAsync(h->d_action, act.data(), sizeof(int) * nd, cudaMemcpyHostToDevice, s));
+        LAUNCH(KT_EPILOGUE, launch_step_state(P, h->substate, s));
+        return DHARA_OK;
+    };
+    for (int st = 0; st < nsteps; ++st) {
+        std::fill(act.begin(), act.end(), 1);
+        int rc = run_actions();
+        if (rc) return rc;
+        std::fill(k.begin(), k.end(), 0);
+        std::fill(rem.begin(), rem.end(), 1LL << K);  // the step in units of dt / 2^K
+        for (;;) {
+            bool left = false;
+            for (int d = 0; d < nd; ++d) left = left || rem[d] > 0;
+            if (!left) break;
+            h->P.n_frozen = 0;
+            for (int d = 0; d < nd; ++d) {
+                DomainDesc &D = h->hdom[d];
+                D.sub_frac = std::ldexp(1.0, -k[d]);
+                D.dt = h->params[d].dt * D.sub_frac;
+                D.step_advance = 0;
+                D.frozen = rem[d] == 0 ? 1 : 0;
+                h->P.n_frozen += D.frozen;
+            }
+            if (upload_dom_desc(h)) return DHARA_ERR_CUDA;
+            rc = enqueue_subsurface(h);
+            if (!rc) rc = enqueue_overland(h);
+            if (rc) return rc;
+            CK(cudaMemcpyAsync(pc.data(), P.pctrl, sizeof(PicardCtrl) * nd, cudaMemcpyDeviceToHost, s));
+            rc = check_device_error(h);  // synchronises
+            if (rc) return rc;
+            for (int d = 0; d < nd; ++d) {
+                if (rem[d] == 0) {
+                    act[d] = 2;
+                    continue;
+                }
+                h->attempts[d] += 1;
+                if (pc[d].converged || k[d] >= h->params[d].dt_halvings) {
+                    rem[d] -= 1LL << (K - k[d]);
+                    h->substeps[d] += 1;
+                    act[d] = 1;
+                } else {
+                    act[d] = 2;
+                    k[d] += 1;
+                }
+            }
+            rc = run_actions();
+            if (rc) return rc;
+        }
+        LAUNCH(KT_EPILOGUE, launch_advance_step(P, s));
+    }
+    h->P.n_frozen = 0;
+    for (int d = 0; d < nd; ++d) {
+        DomainDesc &D = h->hdom[d];
+        D.sub_frac = 1.0;
+        D.dt = h->params[d].dt;
+        D.step_advance = 1;
+        D.frozen = 0;
+    }
+    if (upload_dom_desc(h)) return DHARA_ERR_CUDA;
+    return DHARA_OK;
+}
+
+}  // namespace
+
 int dhara_step(dhara_handle *h, int nsteps, int use_graph) {
     if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
     if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
     if (nsteps < 0) return fail(DHARA_ERR_INVALID, "nsteps < 0");
     if (set_dev(h)) return DHARA_ERR_CUDA;
+    if (h->max_halvings > 0) return step_halving(h, nsteps);
+    for (int d = 0; d < h->ndom; ++d) {
+        h->substeps[d] += nsteps;
+        h->attempts[d] += nsteps;
+    }
     if (use_graph && !h->timing && !h->graph_failed && !h->graph_exec) {
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -1176,6 +1287,8 @@ int dhara_get_diagnostics(dhara_handle *h, int domain, dhara_diagnostics *out) {
     int rc = check_device_error(h);
     std::memset(out, 0, sizeof(*out));
     out->steps = pc.step;
+    out->substeps_total = h->substeps[domain];
+    out->step_attempts_total = h->attempts[domain];
     out->picard_iters_total = dg.picard_iters_total;
     out->krylov_iters_total = dg.krylov_iters_total;
     out->refine_iters_total = dg.refine_iters_total;
@@ -1337,6 +1450,7 @@ int dhara_adjoint(dhara_handle *h, const dhara_adjoint_desc *desc, double *loss,
                     (int)sizeof(dhara_adjoint_desc));
     if (h->ndom != 1) return fail(DHARA_ERR_UNSUPPORTED, "the adjoint runs on single-domain handles");
     if (h->any_dirichlet) return fail(DHARA_ERR_UNSUPPORTED, "the adjoint does not cover Dirichlet faces");
+    if (h->max_halvings > 0) return fail(DHARA_ERR_UNSUPPORTED, "the adjoint does not cover dt_halvings");
     if (!h->prepared) return fail(DHARA_ERR_STATE, "dhara_prepare has not been called");
     if (desc->nsteps < 1 || desc->checkpoint_every < 1 || !desc->theta_target || !desc->q_target)
         return fail(DHARA_ERR_INVALID, "adjoint: need nsteps >= 1, checkpoint_every >= 1 and both targets");

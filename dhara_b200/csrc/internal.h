@@ -78,6 +78,15 @@ struct DomainDesc {
     double alpha, n, theta_s, theta_r, porosity, Ss, am;
     double delta, hmin, K0, sec;
     double picard_tol, krylov_tol, inner_tol, overland_tol;
+    // time-step halving (dt_halvings): dt above is the length of the step
+    // being attempted; sub_frac its share of the full step (the rain of a
+    // step is spread in proportion), step_advance 0 while sub-stepping (the
+    // host advances the step counter once the full step is done), frozen 1
+    // for a domain that has finished the step while others still sub-step
+    // (its Picard iteration and overland solve are skipped; the host restores
+    // its state after the round)
+    double sub_frac;
+    int step_advance, frozen;
 };
 
 struct TileDesc {
@@ -230,6 +239,7 @@ struct DevPtrs {
     int mg_lchunk[MG_MAXLEV + 2];
     int mg_lg;           // levels run as grid phases: the largest lc of any domain
     int mg_nchunk0;      // level-0 chunks (every domain with an interior)
+    int n_frozen;        // domains with DomainDesc::frozen set (time-step halving)
     long long mg_nc;     // coarse points of all domains and levels
     double *mg_a;        // [5][mg_nc]: C, E, N, NE, NW of every coarse row
     double *mg_w, *mg_b, *mg_x, *mg_t;  // [mg_nc] 1/smoother weight, rhs, pre- and post-smoothed
@@ -290,6 +300,16 @@ cudaError_t launch_dirichlet(const DevPtrs &P, const LaunchCfg &L, cudaStream_t 
 cudaError_t launch_picard_check(const DevPtrs &P, cudaStream_t s);
 cudaError_t launch_epilogue(const DevPtrs &P, const LaunchCfg &L, cudaStream_t s);
 cudaError_t launch_eval_fields(const DevPtrs &P, int which, double *out, cudaStream_t s);
+// Saves (action 1) or restores (action 2) each domain's step state -- psi^n,
+// theta^n, K_top, ponding, depth, elevation and its diagnostics -- to or from
+// the copy in S; a restore also resets the Picard and Krylov initial guesses.
+struct StepState {
+    double *psin, *thetan, *ktop, *ph, *h, *H;
+    DevDiag *diag;
+    const int *action;  // [ndom]
+};
+cudaError_t launch_step_state(const DevPtrs &P, const StepState &S, cudaStream_t s);
+cudaError_t launch_advance_step(const DevPtrs &P, cudaStream_t s);
 cudaError_t launch_overland_setup(const DevPtrs &P, long long ctot, cudaStream_t s);
 cudaError_t launch_overland_solve(const DevPtrs &P, const LaunchCfg &L, long long ctot, cudaStream_t s);
 cudaError_t launch_overland_finish(const DevPtrs &P, long long ctot, cudaStream_t s);

@@ -393,8 +393,8 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
     // ---- S0: r = b - A x, b.b and r.r partials, z = W^-1 r; level-1 operators
     if (blockIdx.x == 0)
         for (int d = tid; d < P.ndom; d += blockDim.x) {
-            P.mgctl[d].active = P.mgd[d].nlev > 0 ? 1 : 0;
-            if (P.mgd[d].nlev == 0) {
+            P.mgctl[d].active = (P.mgd[d].nlev > 0 && !P.dom[d].frozen) ? 1 : 0;
+            if (!P.mgctl[d].active) {
                 P.octrl[d].iter = 0;
                 P.octrl[d].rr = 0.0;
                 P.octrl[d].bb = 0.0;

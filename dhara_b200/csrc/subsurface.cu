@@ -96,12 +96,12 @@ __device__ __forceinline__ void prologue_tile(const DevPtrs &P, int tile) {
             P.gctrl->n_active = 0;
             P.gctrl->n_inner_active = 0;
             P.gctrl->n_olf_active = 0;
-            P.gctrl->n_picard = P.ndom;
+            P.gctrl->n_picard = P.ndom - P.n_frozen;
         }
         if (tile == D.tile_begin) {
             PicardCtrl &pc = P.pctrl[td.dom];
             pc.iter = 0;
-            pc.done = 0;
+            pc.done = D.frozen;
             pc.converged = 0;
             pc.err = 0.0;
             P.diag[td.dom].krylov_iters_last = 0;
@@ -120,7 +120,8 @@ __device__ __forceinline__ void prologue_tile(const DevPtrs &P, int tile) {
             ppt = P.ppt[c];
         P.ppt[c] = ppt;
         const double ph = P.ph[c];
-        const double hpoten = ph + ppt / 1000 - P.esoil[c] * D.sec * dt;
+        // the step's rain (mm) spread over its sub-steps (sub_frac 1 without halving)
+        const double hpoten = ph + ppt * D.sub_frac / 1000 - P.esoil[c] * D.sec * dt;
         const double ks = P.ksat[g];
         double qcapa = -P.ktop[c] * ((P.psin[g] - hpoten - 0.5 * dz) / (0.5 * dz));
         // which branches the selection took, each comparison in three states (band3)
@@ -1223,7 +1224,7 @@ __device__ __forceinline__ void epilogue_tile(const DevPtrs &P, int tile) {
         v[3] += (qb - qt) * dt;
         v[5] += qt * dt;
         v[6] += qb * dt;
-        v[7] += P.ppt[cr.c] / 1000.0;
+        v[7] += P.ppt[cr.c] * D.sub_frac / 1000.0;
         // infiltration / ponding, then waterdepth <- ph
         const double ph = fmax(P.hpoten[cr.c] - qt * dt, 0.0);
         P.ph[cr.c] = ph;
@@ -1249,7 +1250,7 @@ __device__ __forceinline__ void epilogue_tile(const DevPtrs &P, int tile) {
         if (!pc.converged) dg.picard_nonconverged += 1;
         if (records(D, BR_PICARD))
             atomicAdd(&dg.branch_sig, branch_mix(pc.step, BR_PICARD, td.dom, (unsigned)pc.iter));
-        pc.step += 1;
+        pc.step += D.step_advance;
     }
 }
 
@@ -1325,7 +1326,53 @@ __global__ void k_eval_fields(DevPtrs P, int which, double *out) {
     }
 }
 
+// Step state save / restore for time-step halving, one block per tile.
+__global__ void __launch_bounds__(TILE_THREADS) k_step_state(DevPtrs P, StepState S) {
+    const TileDesc td = P.tiles[blockIdx.x];
+    const int act = S.action[td.dom];
+    if (act == 0) return;
+    const bool save = act == 1;
+    const DomainDesc &D = P.dom[td.dom];
+    if (blockIdx.x == D.tile_begin && threadIdx.x == 0) {
+        if (save) S.diag[td.dom] = P.diag[td.dom];
+        else P.diag[td.dom] = S.diag[td.dom];
+    }
+    const ColumnRef cr = column_of(P, blockIdx.x);
+    if (!cr.valid) return;
+    auto mv = [&](double *handle, double *copy, long long i) {
+        if (save) copy[i] = handle[i];
+        else handle[i] = copy[i];
+    };
+    mv(P.ktop, S.ktop, cr.c);
+    mv(P.ph, S.ph, cr.c);
+    mv(P.h, S.h, cr.c);
+    mv(P.H, S.H, cr.c);
+    long long g = cr.g0;
+    for (int k = 0; k < cr.nz; ++k, g += cr.sxy) {
+        mv(P.psin, S.psin, g);
+        mv(P.thetan, S.thetan, g);
+        if (!save) {
+            P.psim[g] = S.psin[g];
+            P.x[g] = S.psin[g];
+        }
+    }
+}
+
+__global__ void k_advance_step(DevPtrs P) {
+    for (int d = threadIdx.x; d < P.ndom; d += blockDim.x) P.pctrl[d].step += 1;
+}
+
 // ------------------------------------------------------------- launchers
+cudaError_t launch_step_state(const DevPtrs &P, const StepState &S, cudaStream_t s) {
+    k_step_state<<<P.ntiles, TILE_THREADS, 0, s>>>(P, S);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advance_step(const DevPtrs &P, cudaStream_t s) {
+    k_advance_step<<<1, 256, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_psi_from_theta(const DevPtrs &P, cudaStream_t s) {
     k_psi_from_theta<<<P.ntiles, TILE_THREADS, 0, s>>>(P);
     return cudaGetLastError();

@@ -122,7 +122,18 @@ typedef struct {
      * grid barrier per iteration, thousands of iterations on stiff systems).
      * Every domain of a handle uses the same solver. */
     int32_t overland_solver;
-    int32_t reserved_i[4];
+    /* Time-step halving when the Picard iteration fails to converge (not the
+     * reference's scheme, which accepts a non-converged step; 0, the default,
+     * keeps it).  With k > 0 a step whose Picard iteration ends at its cap is
+     * undone and retried as two steps of dt/2, each of which may halve again,
+     * down to dt/2^k, whose last attempt is accepted whatever its Picard
+     * outcome.  Rain of a step is spread over its sub-steps in proportion to
+     * their length.  Decided per domain: in a batch only the domains that fail
+     * take sub-steps (the others are left at the end of their step).  Steps
+     * run eagerly (no CUDA graph), with one host synchronisation per round of
+     * attempts; layer statistics are not available in this mode. */
+    int32_t dt_halvings;
+    int32_t reserved_i[3];
     double reserved_d[8];
 } dhara_params;
 
@@ -208,7 +219,11 @@ typedef struct {
      * everywhere, so a finite difference between them differentiates one
      * smooth piece.  0 when not recorded. */
     uint64_t branch_signature;
-    double reserved[5];
+    /* accepted steps and sub-steps (dt_halvings), and all attempts including
+     * the undone ones; equal to steps when no step was halved */
+    int64_t substeps_total;
+    int64_t step_attempts_total;
+    double reserved[3];
 } dhara_diagnostics;
 
 /* ---- lifetime ---------------------------------------------------------- */
