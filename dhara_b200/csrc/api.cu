@@ -1183,6 +1183,10 @@ int step_halving(dhara_handle *h, int nsteps) {
                 DomainDesc &D = h->hdom[d];
                 D.sub_frac = std::ldexp(1.0, -k[d]);
                 D.dt = h->params[d].dt * D.sub_frac;
+                // ||b|| of the 3D system grows as 1/dt (the storage term), so the
+                // relative tolerance shrinks with the sub-step to keep the water
+                // a step's solves may leave unbalanced the same
+                D.krylov_tol = h->params[d].krylov_tol * D.sub_frac;
                 D.step_advance = 0;
                 D.frozen = rem[d] == 0 ? 1 : 0;
                 h->P.n_frozen += D.frozen;
@@ -1219,6 +1223,7 @@ int step_halving(dhara_handle *h, int nsteps) {
         DomainDesc &D = h->hdom[d];
         D.sub_frac = 1.0;
         D.dt = h->params[d].dt;
+        D.krylov_tol = h->params[d].krylov_tol;
         D.step_advance = 1;
         D.frozen = 0;
     }

@@ -157,7 +157,8 @@ struct OlfSegState {
 // level halves every dimension that still has at least 3 points, vertex-
 // centred (coarse point I sits on fine point 2I+1), down to at most 2 x 2.
 #define MG_MAXLEV 16
-#define MG_BLOCK_PTS 4096    // levels of at most this many points run in the domain's own block
+#define MG_SMEM_PTS 1536     // a domain's coarsest levels, up to this many points together, run in one block
+#define MG_SMEM_BYTES (MG_SMEM_PTS * 9 * 8)  // their operators, weights and vectors in shared memory
 #define MG_COARSE_SWEEPS 7   // smoothing sweeps on the coarsest level (odd: the result ends in t)
 struct MgDom {
     int nlev;                      // levels; 0 when the domain has no interior cell

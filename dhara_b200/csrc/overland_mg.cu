@@ -28,9 +28,9 @@
 // level -- is a fixed symmetric positive definite operator, as CG needs.
 //
 // Schedule: one persistent cooperative launch per solve for all domains.
-// Levels with more than MG_BLOCK_PTS points run as grid phases over chunks of
-// OLF_THREADS points, one grid barrier each; a domain's smaller levels run in
-// one block with block barriers.  The residual is fused into the restriction
+// A domain's coarsest levels, as many as fit MG_SMEM_PTS points together, run
+// in one block out of shared memory with block barriers; the finer ones run
+// as grid phases over chunks of OLF_THREADS points, one grid barrier each.  The residual is fused into the restriction
 // and the prolongation into the post-smoothing (each point recomputes the few
 // neighbour values it needs), so a grid level costs one barrier on the way
 // down and one on the way up; and with q = A z + beta q the CG updates p and q
@@ -149,15 +149,18 @@ __device__ __forceinline__ Row9 row_of(const DevPtrs &P, const DomainDesc &D, lo
     return r;
 }
 
-// (A v)(i, j) on level l.
+// (A v)(i, j) on level l.  The loads are predicated on the position, not on
+// the coefficients, so all of a row's loads can be in flight at once; level
+// 0's 5-point rows skip the corners.
 __device__ __forceinline__ double apply_row(const Row9 &r, const double *x, const Lvl &v, int i, int j) {
     double s = 0.0;
 #pragma unroll
     for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
         for (int dx = -1; dx <= 1; ++dx) {
-            const double a = r.a[dy + 1][dx + 1];
-            if (a != 0.0) s += a * __ldcg(x + v.at(i + dx, j + dy));
+            if (v.fine && dx != 0 && dy != 0) continue;
+            const bool in = i + dx >= 0 && i + dx < v.m && j + dy >= 0 && j + dy < v.n;
+            if (in) s += r.a[dy + 1][dx + 1] * __ldcg(x + v.at(i + dx, j + dy));
         }
     return s;
 }
@@ -221,68 +224,97 @@ __device__ __forceinline__ void weight_point(const DevPtrs &P, const DomainDesc 
     P.mg_w[v.at(i, j)] = smoother_inv(row_of(P, D, ctot, g, l, v, i, j));
 }
 
-// Level l+1 point (I, J): b = P^T (b_l - A_l x_l), x = W^-1 b.
+// Child a (0, 1, 2 = 2I, 2I+1, 2I+2) of coarse index I along a halved
+// dimension, or I itself (a = 1) along one that is not; weight 0 for none.
+__device__ __forceinline__ void child(int I, int a, bool halves, int mf, int &f, double &w) {
+    if (halves) {
+        f = 2 * I + a;
+        w = f < mf ? (a == 1 ? 1.0 : 0.5) : 0.0;
+    } else {
+        f = I;
+        w = a == 1 ? 1.0 : 0.0;
+    }
+}
+
+// Parents p0, p1 of fine index i along one dimension with weights u0, u1 (0
+// for none): the coarse point on i, or the two beside it.
+__device__ __forceinline__ void parents2(int i, bool halves, int mc, int &p0, double &u0, int &p1, double &u1) {
+    if (!halves) {
+        p0 = p1 = i;
+        u0 = 1.0;
+        u1 = 0.0;
+    } else if (i & 1) {
+        p0 = p1 = (i - 1) >> 1;
+        u0 = 1.0;
+        u1 = 0.0;
+    } else {
+        p0 = (i >> 1) - 1;
+        u0 = p0 >= 0 ? 0.5 : 0.0;
+        p1 = i >> 1;
+        u1 = p1 < mc ? 0.5 : 0.0;
+    }
+}
+
+// (P t)(i, j): level l+1's t interpolated to level l's point (i, j).
+__device__ __forceinline__ double prolong_at(const MgDom &g, int l, const Lvl &c, const double *tc, int i, int j) {
+    int px0, px1, py0, py1;
+    double ux0, ux1, uy0, uy1;
+    parents2(i, g.hx[l], c.m, px0, ux0, px1, ux1);
+    parents2(j, g.hy[l], c.n, py0, uy0, py1, uy1);
+    double s = 0.0;
+    if (ux0 != 0.0 && uy0 != 0.0) s += ux0 * uy0 * __ldcg(tc + c.at(px0, py0));
+    if (ux1 != 0.0 && uy0 != 0.0) s += ux1 * uy0 * __ldcg(tc + c.at(px1, py0));
+    if (ux0 != 0.0 && uy1 != 0.0) s += ux0 * uy1 * __ldcg(tc + c.at(px0, py1));
+    if (ux1 != 0.0 && uy1 != 0.0) s += ux1 * uy1 * __ldcg(tc + c.at(px1, py1));
+    return s;
+}
+
+// Grid levels (one barrier per level each way): level l+1 point (I, J) gets
+// b = P^T (b_l - A_l x_l) with the residual formed at its children, and
+// x = W^-1 b.
 __device__ void restrict_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int I,
                                int J) {
     const Lvl f = level(g, l), c = level(g, l + 1);
-    const LvlVec vf = vectors(P, l), vc = vectors(P, l + 1);
-    int fx[3], fy[3];
-    double wx[3], wy[3];
-    const int nfx = children(I, g.hx[l], f.m, fx, wx), nfy = children(J, g.hy[l], f.n, fy, wy);
+    const LvlVec vf = vectors(P, l);
     double acc = 0.0;
-    for (int b = 0; b < nfy; ++b)
-        for (int a = 0; a < nfx; ++a) {
-            const Row9 r = row_of(P, D, ctot, g, l, f, fx[a], fy[b]);
-            const double res = __ldcg(vf.b + f.at(fx[a], fy[b])) - apply_row(r, vf.x, f, fx[a], fy[b]);
-            acc += wx[a] * wy[b] * res;
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            int fx, fy;
+            double wx, wy;
+            child(I, a, g.hx[l], f.m, fx, wx);
+            child(J, b, g.hy[l], f.n, fy, wy);
+            if (wx == 0.0 || wy == 0.0) continue;
+            const Row9 r = row_of(P, D, ctot, g, l, f, fx, fy);
+            acc += wx * wy * (__ldcg(vf.b + f.at(fx, fy)) - apply_row(r, vf.x, f, fx, fy));
         }
     const long long at = c.at(I, J);
     P.mg_b[at] = acc;
     P.mg_x[at] = winv_at(P, D, ctot, g, l + 1, c, I, J) * acc;
 }
 
-// x_l + P final_{l+1} at (i, j).
-__device__ __forceinline__ double prolonged(const MgDom &g, int l, const Lvl &f, const Lvl &c, const double *x,
-                                            const double *tc, int i, int j) {
-    int px[2], py[2];
-    double ux[2], uy[2];
-    const int npx = parents(i, g.hx[l], c.m, px, ux), npy = parents(j, g.hy[l], c.n, py, uy);
-    double s = __ldcg(x + f.at(i, j));
-    for (int q = 0; q < npy; ++q)
-        for (int p = 0; p < npx; ++p) s += ux[p] * uy[q] * __ldcg(tc + c.at(px[p], py[q]));
-    return s;
-}
-
-// Level l point (i, j): t = x' + W^-1 (b - A x') with x' = x_l + P t_{l+1}.
+// ... and on the way up level l point (i, j) gets t = x' + W^-1 (b - A x')
+// with x' = x_l + P t_{l+1} formed at the point and its neighbours.
 __device__ void smooth_up_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int i,
                                 int j) {
     const Lvl f = level(g, l), c = level(g, l + 1);
     const LvlVec vf = vectors(P, l);
-    const double *tc = P.mg_t;
     const Row9 r = row_of(P, D, ctot, g, l, f, i, j);
     double ax = 0.0, xc = 0.0;
 #pragma unroll
     for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
         for (int dx = -1; dx <= 1; ++dx) {
-            const double a = r.a[dy + 1][dx + 1];
-            if (a == 0.0) continue;
-            const double xp = prolonged(g, l, f, c, vf.x, tc, i + dx, j + dy);
-            ax += a * xp;
+            if (f.fine && dx != 0 && dy != 0) continue;
+            const int ni = i + dx, nj = j + dy;
+            if (ni < 0 || ni >= f.m || nj < 0 || nj >= f.n) continue;
+            const double xp = __ldcg(vf.x + f.at(ni, nj)) + prolong_at(g, l, c, P.mg_t, ni, nj);
+            ax += r.a[dy + 1][dx + 1] * xp;
             if (dx == 0 && dy == 0) xc = xp;
         }
     const long long at = f.at(i, j);
     vf.t[at] = xc + winv_at(P, D, ctot, g, l, f, i, j) * (__ldcg(vf.b + at) - ax);
-}
-
-// One Jacobi sweep on level l from `from` into `to`.
-__device__ __forceinline__ void sweep_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g,
-                                            int l, const double *from, double *to, int i, int j) {
-    const Lvl v = level(g, l);
-    const Row9 r = row_of(P, D, ctot, g, l, v, i, j);
-    const long long at = v.at(i, j);
-    const double b = __ldcg(vectors(P, l).b + at);
-    to[at] = __ldcg(from + at) + winv_at(P, D, ctot, g, l, v, i, j) * (b - apply_row(r, from, v, i, j));
 }
 
 // ----------------------------------------------------------- block levels
@@ -306,26 +338,167 @@ __device__ void block_setup(const DevPtrs &P, const DomainDesc &D, long long cto
     }
 }
 
-// The domain's block levels of a V-cycle: from x_lc = W^-1 b_lc (already
-// formed) down to the coarsest level, its sweeps, and back up; the result of
-// level lc is left in its t vector.
-__device__ void block_vcycle(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g) {
+// The domain's block levels of a V-cycle run in shared memory: each level's
+// stored operator (C, E, N, NE, NW; level 0 as the same five from its
+// 5-point rows), smoother weights and vectors b, x, t, levels packed one after
+// another (the host picks lc so that levels lc .. nlev-1 fit MG_SMEM_PTS).
+// Loaded once per cycle; from x_lc = W^-1 b_lc (already formed) down to the
+// coarsest level, its sweeps, and back up; level lc's result goes back to its
+// t vector in global memory.
+struct SmemMG {
+    double *a[5], *w, *b, *x, *t;
+};
+
+__device__ __forceinline__ SmemMG smem_mg(double *base) {
+    SmemMG S;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) S.a[k] = base + (size_t)k * MG_SMEM_PTS;
+    S.w = base + 5 * (size_t)MG_SMEM_PTS;
+    S.b = base + 6 * (size_t)MG_SMEM_PTS;
+    S.x = base + 7 * (size_t)MG_SMEM_PTS;
+    S.t = base + 8 * (size_t)MG_SMEM_PTS;
+    return S;
+}
+
+struct SL {
+    int m, n, o;  // points and first slot of the level
+    __device__ __forceinline__ int at(int i, int j) const { return o + j * m + i; }
+};
+
+__device__ __forceinline__ Row9 s_row(const SmemMG &S, const SL &v, int i, int j) {
+    Row9 r;
+    const bool w = i > 0, ea = i < v.m - 1, s = j > 0, no = j < v.n - 1;
+    r.a[1][1] = S.a[0][v.at(i, j)];
+    r.a[1][2] = ea ? S.a[1][v.at(i, j)] : 0.0;
+    r.a[1][0] = w ? S.a[1][v.at(i - 1, j)] : 0.0;
+    r.a[2][1] = no ? S.a[2][v.at(i, j)] : 0.0;
+    r.a[0][1] = s ? S.a[2][v.at(i, j - 1)] : 0.0;
+    r.a[2][2] = (ea && no) ? S.a[3][v.at(i, j)] : 0.0;
+    r.a[0][0] = (w && s) ? S.a[3][v.at(i - 1, j - 1)] : 0.0;
+    r.a[2][0] = (w && no) ? S.a[4][v.at(i, j)] : 0.0;
+    r.a[0][2] = (ea && s) ? S.a[4][v.at(i + 1, j - 1)] : 0.0;
+    return r;
+}
+
+__device__ __forceinline__ double s_apply(const Row9 &r, const double *x, const SL &v, int i, int j) {
+    double s = 0.0;
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+            const bool in = i + dx >= 0 && i + dx < v.m && j + dy >= 0 && j + dy < v.n;
+            if (in) s += r.a[dy + 1][dx + 1] * x[v.at(i + dx, j + dy)];
+        }
+    return s;
+}
+
+template <typename Fn>
+__device__ __forceinline__ void s_points(const SL &v, Fn fn) {
+    const int tot = v.m * v.n;
+    for (int p = threadIdx.x; p < tot; p += blockDim.x) fn(p % v.m, p / v.m);
+}
+
+__device__ void block_vcycle(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, double *smem) {
+    const SmemMG S = smem_mg(smem);
+    SL lv[MG_MAXLEV];
+    int o = 0;
+    for (int l = g.lc; l < g.nlev; ++l) {
+        lv[l] = SL{g.m[l], g.n[l], o};
+        o += g.m[l] * g.n[l];
+    }
+    // ---- load the operators, weights and the top level's b and x
+    for (int l = g.lc; l < g.nlev; ++l) {
+        const SL v = lv[l];
+        const Lvl gl = level(g, l);
+        s_points(v, [&](int i, int j) {
+            const int q = v.at(i, j);
+            const long long at = gl.at(i, j);
+            if (l == 0) {
+                const OlfCoef cf = olf_coef(P, D, at, ctot);
+                S.a[0][q] = cf.dg;
+                S.a[1][q] = -cf.ce;
+                S.a[2][q] = -cf.cn;
+                S.a[3][q] = 0.0;
+                S.a[4][q] = 0.0;
+                S.w[q] = 0.8 / cf.dg;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) S.a[k][q] = __ldcg(P.mg_a + (size_t)k * P.mg_nc + at);
+                S.w[q] = __ldcg(P.mg_w + at);
+            }
+            if (l == g.lc) {
+                const LvlVec gv = vectors(P, l);
+                S.b[q] = __ldcg(gv.b + at);
+                S.x[q] = __ldcg(gv.x + at);
+            }
+        });
+    }
+    // ---- down
     for (int l = g.lc; l + 1 < g.nlev; ++l) {
+        const SL f = lv[l], c = lv[l + 1];
         __syncthreads();
-        block_points(g, l + 1, [&](int I, int J) { restrict_point(P, D, ctot, g, l, I, J); });
+        s_points(f, [&](int i, int j) { S.t[f.at(i, j)] = S.b[f.at(i, j)] - s_apply(s_row(S, f, i, j), S.x, f, i, j); });
+        __syncthreads();
+        s_points(c, [&](int I, int J) {
+            double acc = 0.0;
+#pragma unroll
+            for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+                for (int aa = 0; aa < 3; ++aa) {
+                    int fx, fy;
+                    double wx, wy;
+                    child(I, aa, g.hx[l], f.m, fx, wx);
+                    child(J, bb, g.hy[l], f.n, fy, wy);
+                    if (wx != 0.0 && wy != 0.0) acc += wx * wy * S.t[f.at(fx, fy)];
+                }
+            const int q = c.at(I, J);
+            S.b[q] = acc;
+            S.x[q] = S.w[q] * acc;
+        });
     }
+    // ---- coarsest level: MG_COARSE_SWEEPS (odd) sweeps, the result in t
     const int L = g.nlev - 1;
-    const LvlVec vL = vectors(P, L);
-    for (int s = 0; s < MG_COARSE_SWEEPS; ++s) {
+    for (int sw = 0; sw < MG_COARSE_SWEEPS; ++sw) {
         __syncthreads();
-        const double *from = (s & 1) ? vL.t : vL.x;
-        double *to = (s & 1) ? vL.x : vL.t;
-        block_points(g, L, [&](int i, int j) { sweep_point(P, D, ctot, g, L, from, to, i, j); });
+        const double *from = (sw & 1) ? S.t : S.x;
+        double *to = (sw & 1) ? S.x : S.t;
+        const SL v = lv[L];
+        s_points(v, [&](int i, int j) {
+            const int q = v.at(i, j);
+            to[q] = from[q] + S.w[q] * (S.b[q] - s_apply(s_row(S, v, i, j), from, v, i, j));
+        });
     }
+    // ---- up: x_l += P t_{l+1}, then t_l = x_l + W^-1 (b_l - A_l x_l)
     for (int l = L - 1; l >= g.lc; --l) {
+        const SL f = lv[l], c = lv[l + 1];
         __syncthreads();
-        block_points(g, l, [&](int i, int j) { smooth_up_point(P, D, ctot, g, l, i, j); });
+        s_points(f, [&](int i, int j) {
+            int px0, px1, py0, py1;
+            double ux0, ux1, uy0, uy1;
+            parents2(i, g.hx[l], c.m, px0, ux0, px1, ux1);
+            parents2(j, g.hy[l], c.n, py0, uy0, py1, uy1);
+            double sum = 0.0;
+            if (ux0 != 0.0 && uy0 != 0.0) sum += ux0 * uy0 * S.t[c.at(px0, py0)];
+            if (ux1 != 0.0 && uy0 != 0.0) sum += ux1 * uy0 * S.t[c.at(px1, py0)];
+            if (ux0 != 0.0 && uy1 != 0.0) sum += ux0 * uy1 * S.t[c.at(px0, py1)];
+            if (ux1 != 0.0 && uy1 != 0.0) sum += ux1 * uy1 * S.t[c.at(px1, py1)];
+            S.x[f.at(i, j)] += sum;
+        });
+        __syncthreads();
+        s_points(f, [&](int i, int j) {
+            const int q = f.at(i, j);
+            S.t[q] = S.x[q] + S.w[q] * (S.b[q] - s_apply(s_row(S, f, i, j), S.x, f, i, j));
+        });
     }
+    __syncthreads();
+    // ---- level lc's result
+    {
+        const SL v = lv[g.lc];
+        const Lvl gl = level(g, g.lc);
+        double *tg = vectors(P, g.lc).t;
+        s_points(v, [&](int i, int j) { tg[gl.at(i, j)] = S.t[v.at(i, j)]; });
+    }
+    __syncthreads();
 }
 
 // ------------------------------------------------------------ domain sums
@@ -367,9 +540,14 @@ __device__ __forceinline__ DomSums decision_sums(const DevPtrs &P, const MgDom &
 
 // --------------------------------------------------------------- the solve
 __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long ctot) {
+    extern __shared__ double s_mg[];  // a domain's block levels (block_vcycle)
     __shared__ double s_sc[2];
     __shared__ int s_flag;
     const int tid = threadIdx.x;
+    // barrier: one counter that every block adds to once per phase (zeroed by
+    // k_olf_setup before every solve)
+    unsigned int epoch = 0;
+    auto sync = [&]() { return counter_sync(&P.gctrl->olf_bar, (++epoch) * gridDim.x, P.barrier); };
     const int Lg = P.mg_lg;
     const int nchunk0 = P.mg_nchunk0;
     double *part = P.mg_part;
@@ -425,7 +603,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             int I, J;
             if (point_of(ch, g, I, J)) galerkin_point(P, D, ctot, g, 0, I, J);
         });
-    if (!grid_sync(P.barrier)) return;
+    if (!sync()) return;
     // ---- set-up of the grid levels: A_l and the weights of level l-1
     for (int l = 2; l <= Lg; ++l) {
         chunks(l, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
@@ -436,37 +614,40 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             int i, j;
             if (ch.lev < g.lc && point_of(ch, g, i, j)) weight_point(P, D, ctot, g, l - 1, i, j);
         });
-        if (!grid_sync(P.barrier)) return;
+        if (!sync()) return;
     }
     // ---- set-up of every domain's block levels
     for (int d = blockIdx.x; d < P.ndom; d += gridDim.x) {
         const MgDom &g = P.mgd[d];
         if (g.nlev > 0) block_setup(P, P.dom[d], ctot, g);
     }
-    if (!grid_sync(P.barrier)) return;
+    if (!sync()) return;
 
     // The stop decision after `it` updates of x, taken in the first phase of a
-    // V-cycle by every block for the domains it works on and by block 0 for
-    // all of them (it records the stops and the number of live domains).
-    auto decide_all = [&](int it) {
-        if (blockIdx.x != 0) return;
-        int live = 0;
-        for (int d = 0; d < P.ndom; ++d) {
-            const MgDom &g = P.mgd[d];
-            if (!active(d)) continue;
-            const DomSums s = decision_sums(P, g, it);
-            if (mg_stop(P.dom[d], it, s.rr, s.bb, s.pq, s.rz)) {
-                if (tid == 0) {
+    // V-cycle: each domain's by block d mod gridDim, which records a stop and
+    // counts the domain live (slot it % 3 of olf_live, read after the
+    // barrier; the slot of it + 2 is cleared here for later), and again by
+    // every block for the domains of its chunks.
+    auto decide_own = [&](int it) {
+        if (blockIdx.x == 0 && tid == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
+        for (int d = blockIdx.x; d < P.ndom; d += gridDim.x) {
+            if (tid == 0) s_flag = active(d) ? 1 : 0;
+            __syncthreads();
+            const bool act = s_flag != 0;
+            __syncthreads();
+            if (!act) continue;
+            const DomSums sm = decision_sums(P, P.mgd[d], it);
+            if (tid == 0) {
+                if (mg_stop(P.dom[d], it, sm.rr, sm.bb, sm.pq, sm.rz)) {
                     P.mgctl[d].active = 0;
                     P.octrl[d].iter = it;
-                    P.octrl[d].rr = s.rr;
-                    P.octrl[d].bb = s.bb;
+                    P.octrl[d].rr = sm.rr;
+                    P.octrl[d].bb = sm.bb;
+                } else {
+                    atomicAdd(&P.gctrl->olf_live[it % 3], 1);
                 }
-            } else {
-                ++live;
             }
         }
-        if (tid == 0) P.gctrl->olf_live[0] = live;
     };
     // (block 0 may clear a domain's flag during this phase, so one thread reads
     // it for the whole block: the block then takes one path)
@@ -488,7 +669,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
     for (int it = 0;; ++it) {
         // ---- down: restriction with the residual fused, grid levels
         for (int l = 0; l < Lg; ++l) {
-            if (l == 0) decide_all(it);
+            if (l == 0) decide_own(it);
             int cd = -1;
             bool cl = false;
             chunks(l + 1, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
@@ -496,29 +677,29 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
                 int I, J;
                 if (go && point_of(ch, g, I, J)) restrict_point(P, D, ctot, g, l, I, J);
             });
-            if (!grid_sync(P.barrier)) return;
-            if (l == 0 && __ldcg(&P.gctrl->olf_live[0]) == 0) return;
+            if (!sync()) return;
+            if (l == 0 && __ldcg(&P.gctrl->olf_live[it % 3]) == 0) return;
         }
         // ---- the domains' block levels
-        if (Lg == 0) decide_all(it);
+        if (Lg == 0) decide_own(it);
         {
             int cd = -1;
             bool cl = false;
             for (int d = blockIdx.x; d < P.ndom; d += gridDim.x) {
                 const MgDom &g = P.mgd[d];
                 const bool go = Lg == 0 ? live_after(d, it, cd, cl) : active(d);
-                if (go && g.nlev > 0) block_vcycle(P, P.dom[d], ctot, g);
+                if (go && g.nlev > 0) block_vcycle(P, P.dom[d], ctot, g, s_mg);
             }
         }
-        if (!grid_sync(P.barrier)) return;
-        if (Lg == 0 && __ldcg(&P.gctrl->olf_live[0]) == 0) return;
+        if (!sync()) return;
+        if (Lg == 0 && __ldcg(&P.gctrl->olf_live[it % 3]) == 0) return;
         // ---- up: prolongation with the post-smoothing fused, grid levels
         for (int l = Lg - 1; l >= 1; --l) {
             chunks(l, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
                 int i, j;
                 if (ch.lev < g.lc && active(ch.dom) && point_of(ch, g, i, j)) smooth_up_point(P, D, ctot, g, l, i, j);
             });
-            if (!grid_sync(P.barrier)) return;
+            if (!sync()) return;
         }
         // ---- level 0: z (the preconditioned residual, in olf_w) and r.z
         chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
@@ -533,7 +714,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             olf_block_sum<1>(v);
             if (tid == 0) pslot(MP_RZ + (it & 1), k) = v[0];
         });
-        if (!grid_sync(P.barrier)) return;
+        if (!sync()) return;
         // ---- X: p = z + beta p, q = A z + beta q, p.q
         {
             int cd = -1;
@@ -566,7 +747,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
                 if (tid == 0) pslot(MP_PQ, k) = pq[0];
             });
         }
-        if (!grid_sync(P.barrier)) return;
+        if (!sync()) return;
         // ---- Y: x += alpha p, r -= alpha q, r.r, z = W^-1 r
         {
             int cd = -1;
@@ -596,7 +777,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
                 if (tid == 0) pslot(MP_RR, k) = rr[0];
             });
         }
-        if (!grid_sync(P.barrier)) return;
+        if (!sync()) return;
     }
 }
 
@@ -630,8 +811,13 @@ void mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::
             nc += (long long)m * n;
         }
         g.nlev = L + 1;
-        g.lc = 0;
-        while (g.lc < g.nlev - 1 && (long long)g.m[g.lc] * g.n[g.lc] > MG_BLOCK_PTS) ++g.lc;
+        // the block levels: the coarsest ones that fit MG_SMEM_PTS together
+        long long tail = 0;
+        g.lc = g.nlev;
+        while (g.lc > 0 && tail + (long long)g.m[g.lc - 1] * g.n[g.lc - 1] <= MG_SMEM_PTS) {
+            --g.lc;
+            tail += (long long)g.m[g.lc] * g.n[g.lc];
+        }
         lg = std::max(lg, g.lc);
     }
     // chunk lists: level 0 for every domain with an interior (the CG's
@@ -657,8 +843,10 @@ cudaError_t configure_mg(LaunchCfg &L, int device) {
     cudaDeviceProp prop;
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute((const void *)k_olf_mgcg, cudaFuncAttributeMaxDynamicSharedMemorySize, MG_SMEM_BYTES);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_mgcg, OLF_THREADS, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_olf_mgcg, OLF_THREADS, MG_SMEM_BYTES);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     L.mg_blocks = per_sm * prop.multiProcessorCount;
@@ -672,5 +860,6 @@ cudaError_t launch_overland_mg(const DevPtrs &P, const LaunchCfg &L, long long c
     int need = P.ndom;
     for (int l = 0; l <= P.mg_lg; ++l) need = std::max(need, P.mg_lchunk[l + 1] - P.mg_lchunk[l]);
     const int grid = std::max(1, std::min(L.mg_blocks, need));
-    return cudaLaunchCooperativeKernel((const void *)k_olf_mgcg, dim3(grid), dim3(OLF_THREADS), kargs, 0, s);
+    return cudaLaunchCooperativeKernel((const void *)k_olf_mgcg, dim3(grid), dim3(OLF_THREADS), kargs, MG_SMEM_BYTES,
+                                       s);
 }

@@ -38,8 +38,16 @@ def mass_error(dg):
     return abs(dg["storage_change_cum"] - (dg["top_inflow_cum"] - dg["bottom_outflow_cum"])) / dg["top_inflow_cum"]
 
 
+def converging_domain():
+    """Light rain (5 mm/h) on a domain whose Picard iteration converges at full
+    dt every step (the oracle needs 52 iterations over the 6 steps, cap 20)."""
+    return inputs.make_domain(24, 20, 12, seed=3, nsteps=6, precision=db.FP64, rain_mm_per_h=5.0,
+                              picard_maxiter=20, picard_rule=db._abi.PICARD_PSI_ABSOLUTE, picard_tol=1e-6,
+                              krylov_tol=1e-10, krylov_maxiter=2000)
+
+
 def test_converging_domain_is_unchanged(gpu):
-    d = inputs.plain_fp64_32x32x20(nsteps=6)
+    d = converging_domain()
     (a, da), = run([d], 6)
     (b, dbb), = run([with_halvings(d, 4)], 6)
     assert da["picard_nonconverged"] == 0
@@ -50,16 +58,18 @@ def test_converging_domain_is_unchanged(gpu):
 
 def test_diverging_domain_stays_bounded(gpu):
     # ensemble domain 20 (16 x 123 x 21, alpha 4.25 /m, n 2.04): under the
-    # reference scheme its Picard iterates diverge within a few steps
+    # reference scheme every step ends at the Picard cap and the heads run
+    # away (hundreds of metres within 12 steps, ~1e9 m later)
     d = inputs.ensemble(256, nsteps=12)[20]
     (a, da), = run([d], 12)
     (b, dbb), = run([with_halvings(d, 10)], 12)
     print("reference scheme: max |psi|", np.abs(a["psi"]).max(), "capped steps", da["picard_nonconverged"])
     print("halving: max |psi|", np.abs(b["psi"]).max(), "capped", dbb["picard_nonconverged"],
           "sub-steps", dbb["substeps_total"], "attempts", dbb["step_attempts_total"], "mass", mass_error(dbb))
-    assert np.abs(a["psi"]).max() > 1e3
-    assert np.abs(b["psi"]).max() < 1e2
-    assert dbb["picard_nonconverged"] < da["picard_nonconverged"]
+    assert da["picard_nonconverged"] == 12 and np.abs(a["psi"]).max() > 1e2
+    assert np.abs(b["psi"]).max() < 5.0
+    # only sub-steps at the smallest length (dt / 1024) may end at the cap
+    assert dbb["picard_nonconverged"] < 0.1 * dbb["substeps_total"]
     assert dbb["steps"] == 12 and dbb["substeps_total"] > 12
     assert mass_error(dbb) < 1e-8
 
