@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=120)
     ap.add_argument("--fd-steps", type=int, default=20)
     ap.add_argument("--ensemble-steps", type=int, default=120)
-    ap.add_argument("--ensemble-halving-steps", type=int, default=30)
+    ap.add_argument("--ensemble-halving-steps", type=int, default=4)
     ap.add_argument("--autotune", type=int, default=1)
     return ap.parse_args()
 
@@ -410,17 +410,20 @@ def run_ensemble(args, local, world=1, rank=0):
 
 
 def run_ensemble_halving(args, local, world=1, rank=0):
-    """The same 256 domains with time-step halving (dt_halvings 8: a step
+    """The same 256 domains with time-step halving (dt_halvings 6: a step
     whose Picard iteration does not converge is redone as two half steps,
-    down to dt/256), the opt-in converging variant of the reference's scheme.
-    The rate counts full steps; the sub-steps and all attempts (undone ones
-    included) are reported beside it."""
+    down to dt/64), the opt-in converging variant of the reference's scheme,
+    over the first steps (a bounded sample: the Picard iteration of the
+    saturated zone stalls at any step length in many of these domains, so
+    most of their sub-steps end at the smallest length).  The rate counts full
+    steps; the sub-steps and all attempts (undone ones included) are reported
+    beside it."""
     from dhara_b200 import ensemble as ens
     from dhara_b200 import inputs
     nsteps = args.ensemble_halving_steps
     doms = inputs.ensemble(256, nsteps=max(nsteps, 1))
     for d in doms:
-        d.params.dt_halvings = 8
+        d.params.dt_halvings = 6
     cells = sum(d.ncells for d in doms)
     barrier(world)
     ms, launches, diags = ens.run_sharded(doms, nsteps, rank, world, device=local, autotune=0)
@@ -436,7 +439,7 @@ def run_ensemble_halving(args, local, world=1, rank=0):
         inflow = dg["top_inflow_cum"]
         if inflow:
             worst_mass = max(worst_mass, abs(dg["storage_change_cum"] - (inflow - dg["bottom_outflow_cum"])) / inflow)
-    return {"workload": "ensemble_256_domains_dt_halving_8", "domains": len(doms), "cells": cells,
+    return {"workload": "ensemble_256_domains_dt_halving_6", "domains": len(doms), "cells": cells,
             "steps": nsteps, "ms_per_step": ms_max / nsteps, "value": cells * nsteps / (ms_max / 1e3),
             "unit": "cell-steps/s (full steps)", "ranks": world, "domain_steps": len(doms) * nsteps,
             "substeps_total": sub, "step_attempts_total": att, "picard_steps_at_cap": capped,

@@ -1914,13 +1914,13 @@ struct CkptHeader {
     int64_t ntot, ctot;
     int32_t pctrl_bytes, diag_bytes;
 };
-constexpr int32_t CKPT_VERSION = 1;
+constexpr int32_t CKPT_VERSION = 2;
 constexpr int CKPT_DIM_INTS = 3;  // nx, ny, nz per domain, after the header
 
 size_t ckpt_bytes(const dhara_handle *h) {
     return sizeof(CkptHeader) + (size_t)h->ndom * CKPT_DIM_INTS * sizeof(int32_t) +
            ((size_t)2 * h->Ntot + (size_t)4 * h->Ctot) * sizeof(double) +
-           (size_t)h->ndom * (sizeof(PicardCtrl) + sizeof(DevDiag));
+           (size_t)h->ndom * (sizeof(PicardCtrl) + sizeof(DevDiag) + 2 * sizeof(int64_t));
 }
 
 // The device arrays of the checkpoint, in buffer order, with their lengths.
@@ -1975,6 +1975,13 @@ int dhara_checkpoint(dhara_handle *h, void *buf, int64_t bytes) {
     CK(cudaMemcpyAsync(q, h->P.pctrl, h->ndom * sizeof(PicardCtrl), cudaMemcpyDeviceToHost, s));
     q += h->ndom * sizeof(PicardCtrl);
     CK(cudaMemcpyAsync(q, h->P.diag, h->ndom * sizeof(DevDiag), cudaMemcpyDeviceToHost, s));
+    q += h->ndom * sizeof(DevDiag);
+    // the accepted sub-step and attempt counts (host side)
+    for (int d = 0; d < h->ndom; ++d) {
+        const int64_t c[2] = {h->substeps[d], h->attempts[d]};
+        std::memcpy(q, c, sizeof(c));
+        q += sizeof(c);
+    }
     CK(cudaStreamSynchronize(s));
     return check_device_error(h);
 }
@@ -2021,6 +2028,14 @@ int dhara_restore(dhara_handle *h, const void *buf, int64_t bytes) {
     CK(cudaMemcpyAsync(P.pctrl, q, h->ndom * sizeof(PicardCtrl), cudaMemcpyHostToDevice, s));
     q += h->ndom * sizeof(PicardCtrl);
     CK(cudaMemcpyAsync(P.diag, q, h->ndom * sizeof(DevDiag), cudaMemcpyHostToDevice, s));
+    q += h->ndom * sizeof(DevDiag);
+    for (int d = 0; d < h->ndom; ++d) {
+        int64_t c[2];
+        std::memcpy(c, q, sizeof(c));
+        q += sizeof(c);
+        h->substeps[d] = c[0];
+        h->attempts[d] = c[1];
+    }
     CK(cudaStreamSynchronize(s));
     return DHARA_OK;
 }
