@@ -149,18 +149,56 @@ __device__ __forceinline__ Row9 row_of(const DevPtrs &P, const DomainDesc &D, lo
     return r;
 }
 
-// (A v)(i, j) on level l.  The loads are predicated on the position, not on
-// the coefficients, so all of a row's loads can be in flight at once; level
-// 0's 5-point rows skip the corners.
-__device__ __forceinline__ double apply_row(const Row9 &r, const double *x, const Lvl &v, int i, int j) {
+// The grid phases' form of row_of: every load is unconditional, at
+// an address clamped into the level (level 0's ring cells exist in memory),
+// and the entries outside the level are selected to zero after the loads, so
+// no load waits on a branch and all of a point's loads can be in flight.
+// FINE: level 0 (5-point rows from the conductances).
+template <bool FINE>
+__device__ __forceinline__ Row9 row_nb(const DevPtrs &P, const DomainDesc &D, long long ctot, const Lvl &v, int i,
+                                       int j) {
+    Row9 r;
+    const bool w = i > 0, ea = i < v.m - 1, s = j > 0, no = j < v.n - 1;
+    if constexpr (FINE) {
+        const OlfCoef cf = olf_coef(P, D, v.at(i, j), ctot);
+        r.a[1][1] = cf.dg;
+        r.a[1][0] = w ? -cf.cw : 0.0;
+        r.a[1][2] = ea ? -cf.ce : 0.0;
+        r.a[0][1] = s ? -cf.cs : 0.0;
+        r.a[2][1] = no ? -cf.cn : 0.0;
+        r.a[0][0] = r.a[0][2] = r.a[2][0] = r.a[2][2] = 0.0;
+    } else {
+        const int im = w ? i - 1 : i, ip = ea ? i + 1 : i, jm = s ? j - 1 : j;
+        const long long nc = P.mg_nc;
+        const double *A = P.mg_a;
+        auto e = [&](int k, int ii, int jj) { return __ldcg(A + (size_t)k * nc + v.at(ii, jj)); };
+        const double c = e(0, i, j), eE = e(1, i, j), eW = e(1, im, j), nN = e(2, i, j), nS = e(2, i, jm);
+        const double neNE = e(3, i, j), neSW = e(3, im, jm), nwNW = e(4, i, j), nwSE = e(4, ip, jm);
+        r.a[1][1] = c;
+        r.a[1][2] = ea ? eE : 0.0;
+        r.a[1][0] = w ? eW : 0.0;
+        r.a[2][1] = no ? nN : 0.0;
+        r.a[0][1] = s ? nS : 0.0;
+        r.a[2][2] = (ea && no) ? neNE : 0.0;
+        r.a[0][0] = (w && s) ? neSW : 0.0;
+        r.a[2][0] = (w && no) ? nwNW : 0.0;
+        r.a[0][2] = (ea && s) ? nwSE : 0.0;
+    }
+    return r;
+}
+
+__device__ __forceinline__ int clampi(int i, int n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
+
+template <bool FINE>
+__device__ __forceinline__ double apply_nb(const Row9 &r, const double *x, const Lvl &v, int i, int j) {
     double s = 0.0;
 #pragma unroll
     for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
         for (int dx = -1; dx <= 1; ++dx) {
-            if (v.fine && dx != 0 && dy != 0) continue;
-            const bool in = i + dx >= 0 && i + dx < v.m && j + dy >= 0 && j + dy < v.n;
-            if (in) s += r.a[dy + 1][dx + 1] * __ldcg(x + v.at(i + dx, j + dy));
+            if (FINE && dx != 0 && dy != 0) continue;  // compile-time: no corners at level 0
+            const int ii = FINE ? i + dx : clampi(i + dx, v.m), jj = FINE ? j + dy : clampi(j + dy, v.n);
+            s += r.a[dy + 1][dx + 1] * __ldcg(x + v.at(ii, jj));
         }
     return s;
 }
@@ -173,12 +211,6 @@ __device__ __forceinline__ double smoother_inv(const Row9 &r) {
 #pragma unroll
         for (int x = 0; x < 3; ++x) l1 += fabs(r.a[y][x]);
     return 1.0 / fmax(r.a[1][1] / 0.8, 0.55 * l1);
-}
-
-__device__ __forceinline__ double winv_at(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g,
-                                          int l, const Lvl &v, int i, int j) {
-    if (l == 0) return 0.8 / olf_coef(P, D, v.at(i, j), ctot).dg;  // the weight is a_ii/0.8 on the M-matrix
-    return __ldcg(P.mg_w + v.at(i, j));
 }
 
 // ---------------------------------------------------------- point kernels
@@ -252,6 +284,8 @@ __device__ __forceinline__ void parents2(int i, bool halves, int mc, int &p0, do
         u0 = p0 >= 0 ? 0.5 : 0.0;
         p1 = i >> 1;
         u1 = p1 < mc ? 0.5 : 0.0;
+        p0 = p0 < 0 ? 0 : p0;  // a parent of weight 0 points at a valid slot
+        p1 = p1 < mc ? p1 : mc - 1;
     }
 }
 
@@ -261,17 +295,17 @@ __device__ __forceinline__ double prolong_at(const MgDom &g, int l, const Lvl &c
     double ux0, ux1, uy0, uy1;
     parents2(i, g.hx[l], c.m, px0, ux0, px1, ux1);
     parents2(j, g.hy[l], c.n, py0, uy0, py1, uy1);
-    double s = 0.0;
-    if (ux0 != 0.0 && uy0 != 0.0) s += ux0 * uy0 * __ldcg(tc + c.at(px0, py0));
-    if (ux1 != 0.0 && uy0 != 0.0) s += ux1 * uy0 * __ldcg(tc + c.at(px1, py0));
-    if (ux0 != 0.0 && uy1 != 0.0) s += ux0 * uy1 * __ldcg(tc + c.at(px0, py1));
-    if (ux1 != 0.0 && uy1 != 0.0) s += ux1 * uy1 * __ldcg(tc + c.at(px1, py1));
-    return s;
+    // every parent slot is valid (weight 0 where there is no parent), so the
+    // four loads are unconditional
+    return (ux0 * uy0 * __ldcg(tc + c.at(px0, py0)) + ux1 * uy0 * __ldcg(tc + c.at(px1, py0))) +
+           (ux0 * uy1 * __ldcg(tc + c.at(px0, py1)) + ux1 * uy1 * __ldcg(tc + c.at(px1, py1)));
 }
 
 // Grid levels (one barrier per level each way): level l+1 point (I, J) gets
 // b = P^T (b_l - A_l x_l) with the residual formed at its children, and
-// x = W^-1 b.
+// x = W^-1 b.  A child outside the level (weight 0) is read at a clamped
+// position, so the nine children's loads do not wait on branches.
+template <bool FINE>
 __device__ void restrict_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int I,
                                int J) {
     const Lvl f = level(g, l), c = level(g, l + 1);
@@ -285,36 +319,39 @@ __device__ void restrict_point(const DevPtrs &P, const DomainDesc &D, long long 
             double wx, wy;
             child(I, a, g.hx[l], f.m, fx, wx);
             child(J, b, g.hy[l], f.n, fy, wy);
-            if (wx == 0.0 || wy == 0.0) continue;
-            const Row9 r = row_of(P, D, ctot, g, l, f, fx, fy);
-            acc += wx * wy * (__ldcg(vf.b + f.at(fx, fy)) - apply_row(r, vf.x, f, fx, fy));
+            fx = clampi(fx, f.m);
+            fy = clampi(fy, f.n);
+            const Row9 r = row_nb<FINE>(P, D, ctot, f, fx, fy);
+            acc += (wx * wy) * (__ldcg(vf.b + f.at(fx, fy)) - apply_nb<FINE>(r, vf.x, f, fx, fy));
         }
     const long long at = c.at(I, J);
     P.mg_b[at] = acc;
-    P.mg_x[at] = winv_at(P, D, ctot, g, l + 1, c, I, J) * acc;
+    P.mg_x[at] = __ldcg(P.mg_w + at) * acc;
 }
 
 // ... and on the way up level l point (i, j) gets t = x' + W^-1 (b - A x')
-// with x' = x_l + P t_{l+1} formed at the point and its neighbours.
+// with x' = x_l + P t_{l+1} formed at the point and its neighbours (clamped
+// positions where a neighbour is outside the level, whose coefficient is 0).
+template <bool FINE>
 __device__ void smooth_up_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int i,
                                 int j) {
     const Lvl f = level(g, l), c = level(g, l + 1);
     const LvlVec vf = vectors(P, l);
-    const Row9 r = row_of(P, D, ctot, g, l, f, i, j);
+    const Row9 r = row_nb<FINE>(P, D, ctot, f, i, j);
     double ax = 0.0, xc = 0.0;
 #pragma unroll
     for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
         for (int dx = -1; dx <= 1; ++dx) {
-            if (f.fine && dx != 0 && dy != 0) continue;
-            const int ni = i + dx, nj = j + dy;
-            if (ni < 0 || ni >= f.m || nj < 0 || nj >= f.n) continue;
+            if (FINE && dx != 0 && dy != 0) continue;  // compile-time: no corners at level 0
+            const int ni = clampi(i + dx, f.m), nj = clampi(j + dy, f.n);
             const double xp = __ldcg(vf.x + f.at(ni, nj)) + prolong_at(g, l, c, P.mg_t, ni, nj);
             ax += r.a[dy + 1][dx + 1] * xp;
             if (dx == 0 && dy == 0) xc = xp;
         }
     const long long at = f.at(i, j);
-    vf.t[at] = xc + winv_at(P, D, ctot, g, l, f, i, j) * (__ldcg(vf.b + at) - ax);
+    const double winv = FINE ? 0.8 / r.a[1][1] : __ldcg(P.mg_w + at);
+    vf.t[at] = xc + winv * (__ldcg(vf.b + at) - ax);
 }
 
 // ----------------------------------------------------------- block levels
@@ -502,17 +539,23 @@ __device__ void block_vcycle(const DevPtrs &P, const DomainDesc &D, long long ct
 }
 
 // ------------------------------------------------------------ domain sums
-// Sums of the given chunk-partial slots over the domain's level-0 chunks, in
-// chunk order (the same bits in every block).
+// Sums of the given chunk-partial slots over the domain's level-0 chunks,
+// taken by each warp on its own (lane k sums chunks k, k+32, ..., then a
+// butterfly), so every warp of every block gets the same bits with no block
+// barrier.
 template <int NV>
 __device__ __forceinline__ void chunk_sums(const DevPtrs &P, const MgDom &g, const int (&slot)[NV], double (&v)[NV]) {
+    const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int i = 0; i < NV; ++i) v[i] = 0.0;
-    for (int k = threadIdx.x; k < g.c0_count; k += blockDim.x) {
+    for (int k = lane; k < g.c0_count; k += 32) {
 #pragma unroll
         for (int i = 0; i < NV; ++i) v[i] += __ldcg(&P.mg_part[(size_t)slot[i] * P.mg_nchunk0 + g.c0_first + k]);
     }
-    olf_block_sum<NV>(v);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
 }
 
 // The CG's stop decision of a domain after `it` updates of x: converged
@@ -541,8 +584,6 @@ __device__ __forceinline__ DomSums decision_sums(const DevPtrs &P, const MgDom &
 // --------------------------------------------------------------- the solve
 __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long ctot) {
     extern __shared__ double s_mg[];  // a domain's block levels (block_vcycle)
-    __shared__ double s_sc[2];
-    __shared__ int s_flag;
     const int tid = threadIdx.x;
     // barrier: one counter that every block adds to once per phase (zeroed by
     // k_olf_setup before every solve)
@@ -631,11 +672,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
     auto decide_own = [&](int it) {
         if (blockIdx.x == 0 && tid == 0) P.gctrl->olf_live[(it + 2) % 3] = 0;
         for (int d = blockIdx.x; d < P.ndom; d += gridDim.x) {
-            if (tid == 0) s_flag = active(d) ? 1 : 0;
-            __syncthreads();
-            const bool act = s_flag != 0;
-            __syncthreads();
-            if (!act) continue;
+            if (!active(d)) continue;  // only this block writes the flag of d
             const DomSums sm = decision_sums(P, P.mgd[d], it);
             if (tid == 0) {
                 if (mg_stop(P.dom[d], it, sm.rr, sm.bb, sm.pq, sm.rz)) {
@@ -649,18 +686,15 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             }
         }
     };
-    // (block 0 may clear a domain's flag during this phase, so one thread reads
-    // it for the whole block: the block then takes one path)
+    // The same decision for a domain this block works on (the owner may clear
+    // the flag during this phase: either value leads to the same outcome).
     auto live_after = [&](int d, int it, int &cache_dom, bool &cache_live) {
         if (d != cache_dom) {
             cache_dom = d;
-            if (tid == 0) s_flag = active(d) ? 1 : 0;
-            __syncthreads();
-            cache_live = s_flag != 0;
-            __syncthreads();
+            cache_live = active(d);
             if (cache_live) {
-                const DomSums s = decision_sums(P, P.mgd[d], it);
-                cache_live = !mg_stop(P.dom[d], it, s.rr, s.bb, s.pq, s.rz);
+                const DomSums sm = decision_sums(P, P.mgd[d], it);
+                cache_live = !mg_stop(P.dom[d], it, sm.rr, sm.bb, sm.pq, sm.rz);
             }
         }
         return cache_live;
@@ -675,7 +709,10 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             chunks(l + 1, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
                 const bool go = l == 0 ? live_after(ch.dom, it, cd, cl) : active(ch.dom);
                 int I, J;
-                if (go && point_of(ch, g, I, J)) restrict_point(P, D, ctot, g, l, I, J);
+                if (go && point_of(ch, g, I, J)) {
+                    if (l == 0) restrict_point<true>(P, D, ctot, g, l, I, J);
+                    else restrict_point<false>(P, D, ctot, g, l, I, J);
+                }
             });
             if (!sync()) return;
             if (l == 0 && __ldcg(&P.gctrl->olf_live[it % 3]) == 0) return;
@@ -697,7 +734,8 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
         for (int l = Lg - 1; l >= 1; --l) {
             chunks(l, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
                 int i, j;
-                if (ch.lev < g.lc && active(ch.dom) && point_of(ch, g, i, j)) smooth_up_point(P, D, ctot, g, l, i, j);
+                if (ch.lev < g.lc && active(ch.dom) && point_of(ch, g, i, j))
+                    smooth_up_point<false>(P, D, ctot, g, l, i, j);
             });
             if (!sync()) return;
         }
@@ -707,7 +745,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             double v[1] = {0.0};
             int i, j;
             if (point_of(ch, g, i, j)) {
-                if (g.lc > 0) smooth_up_point(P, D, ctot, g, 0, i, j);
+                if (g.lc > 0) smooth_up_point<true>(P, D, ctot, g, 0, i, j);
                 const long long c = level(g, 0).at(i, j);
                 v[0] = __ldcg(P.olf_r + c) * __ldcg(P.olf_w + c);
             }
@@ -718,6 +756,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
         // ---- X: p = z + beta p, q = A z + beta q, p.q
         {
             int cd = -1;
+            double beta = 0.0;
             chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
                 if (!active(ch.dom)) return;
                 if (ch.dom != cd) {
@@ -725,10 +764,8 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
                     const int slots[2] = {MP_RZ + (it & 1), MP_RZ + ((it + 1) & 1)};
                     double v[2];
                     chunk_sums<2>(P, g, slots, v);
-                    if (tid == 0) s_sc[0] = it == 0 ? 0.0 : v[0] / v[1];
-                    __syncthreads();
+                    beta = it == 0 ? 0.0 : v[0] / v[1];
                 }
-                const double beta = s_sc[0];
                 double pq[1] = {0.0};
                 int i, j;
                 if (point_of(ch, g, i, j)) {
@@ -751,6 +788,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
         // ---- Y: x += alpha p, r -= alpha q, r.r, z = W^-1 r
         {
             int cd = -1;
+            double alpha = 0.0;
             chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
                 if (!active(ch.dom)) return;
                 if (ch.dom != cd) {
@@ -758,10 +796,8 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
                     const int slots[2] = {MP_RZ + (it & 1), MP_PQ};
                     double v[2];
                     chunk_sums<2>(P, g, slots, v);
-                    if (tid == 0) s_sc[1] = (v[1] > 0.0 && v[0] > 0.0 && v[1] < 1e300) ? v[0] / v[1] : 0.0;
-                    __syncthreads();
+                    alpha = (v[1] > 0.0 && v[0] > 0.0 && v[1] < 1e300) ? v[0] / v[1] : 0.0;
                 }
-                const double alpha = s_sc[1];
                 double rr[1] = {0.0};
                 int i, j;
                 if (point_of(ch, g, i, j)) {
