@@ -681,6 +681,10 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         if (p.nz > h->nz_max) h->nz_max = p.nz;
         if (p.picard_maxiter > h->maxiter_picard) h->maxiter_picard = p.picard_maxiter;
     }
+    // the inner sweeps index cells with 32-bit offsets
+    if (h->Ntot >= (1LL << 31))
+        return bail(fail(DHARA_ERR_UNSUPPORTED, "a handle holds at most 2^31 - 1 cells (with row padding); got %lld",
+                         (long long)h->Ntot));
     // tile lists: room for either shape's list, the per-domain plan by default
     for (int d = 0; d < ndomains; ++d)
         h->tiles_cap += std::max(tile_count(h->hdom[d], TILE_X, TILE_Y), tile_count(h->hdom[d], 16, 8));

@@ -160,6 +160,7 @@ struct OlfSegState {
 #define MG_SMEM_PTS 1536     // a domain's coarsest levels, up to this many points together, run in one block
 #define MG_SMEM_BYTES (MG_SMEM_PTS * 9 * 8)  // their operators, weights and vectors in shared memory
 #define MG_COARSE_SWEEPS 7   // smoothing sweeps on the coarsest level (odd: the result ends in t)
+#define MG_CHUNK0 (4 * OLF_THREADS)  // points of a level-0 chunk (the CG's vectors), four per thread
 struct MgDom {
     int nlev;                      // levels; 0 when the domain has no interior cell
     int lc;                        // first level run by the domain's block (levels lc .. nlev-1)
@@ -169,7 +170,8 @@ struct MgDom {
     unsigned char hx[MG_MAXLEV], hy[MG_MAXLEV]; // level l+1 halves x (y) of level l
     long long off[MG_MAXLEV];      // level 0: the domain's surface offset; else first coarse point
 };
-// A run of up to OLF_THREADS consecutive points of one level of one domain.
+// A run of up to OLF_THREADS (level 0: MG_CHUNK0) consecutive points of one
+// level of one domain.
 struct MgChunk {
     int dom, lev, first, count;
 };

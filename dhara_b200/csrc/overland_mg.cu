@@ -27,7 +27,9 @@
 // correction, post-smoothing, and MG_COARSE_SWEEPS sweeps on the coarsest
 // level -- is a fixed symmetric positive definite operator, as CG needs.
 //
-// Schedule: one persistent cooperative launch per solve for all domains.
+// Schedule: one persistent cooperative launch per solve for all domains
+// (level-0 work in chunks of MG_CHUNK0 points, four per thread; coarser
+// levels one point per thread).
 // A domain's coarsest levels, as many as fit MG_SMEM_PTS points together, run
 // in one block out of shared memory with block barriers; the finer ones run
 // as grid phases over chunks of OLF_THREADS points, one grid barrier each.  The residual is fused into the restriction
@@ -548,6 +550,7 @@ __device__ __forceinline__ void chunk_sums(const DevPtrs &P, const MgDom &g, con
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int i = 0; i < NV; ++i) v[i] = 0.0;
+#pragma unroll 8
     for (int k = lane; k < g.c0_count; k += 32) {
 #pragma unroll
         for (int i = 0; i < NV; ++i) v[i] += __ldcg(&P.mg_part[(size_t)slot[i] * P.mg_nchunk0 + g.c0_first + k]);
@@ -607,6 +610,17 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
         j = p / g.m[ch.lev];
         return true;
     };
+    // the points of a level-0 chunk (MG_CHUNK0 = 4 per thread)
+    auto points0 = [&](const MgChunk &ch, const MgDom &g, auto fn) {
+#pragma unroll
+        for (int q = 0; q < MG_CHUNK0 / OLF_THREADS; ++q) {
+            const int o = tid + q * OLF_THREADS;
+            if (o < ch.count) {
+                const int p = ch.first + o;
+                fn(p % g.m[0], p / g.m[0]);
+            }
+        }
+    };
     auto active = [&](int d) { return __ldcg(&P.mgctl[d].active) != 0; };
 
     // ---- S0: r = b - A x, b.b and r.r partials, z = W^-1 r; level-1 operators
@@ -621,8 +635,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
         }
     chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
         double v[2] = {0.0, 0.0};
-        int i, j;
-        if (point_of(ch, g, i, j)) {
+        points0(ch, g, [&](int i, int j) {
             const Lvl f = level(g, 0);
             const long long c = f.at(i, j);
             const OlfCoef cf = olf_coef(P, D, c, ctot);
@@ -630,9 +643,9 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             const double r = b - olf_av<false>(cf, P.H, c, f.nx, P.H[c]);
             P.olf_r[c] = r;
             P.olf_z[c] = 0.8 / cf.dg * r;
-            v[0] = r * r;
-            v[1] = b * b;
-        }
+            v[0] += r * r;
+            v[1] += b * b;
+        });
         olf_block_sum<2>(v);
         if (tid == 0) {
             pslot(MP_RR, k) = v[0];
@@ -743,12 +756,11 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
         chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
             if (!active(ch.dom)) return;
             double v[1] = {0.0};
-            int i, j;
-            if (point_of(ch, g, i, j)) {
+            points0(ch, g, [&](int i, int j) {
                 if (g.lc > 0) smooth_up_point<true>(P, D, ctot, g, 0, i, j);
                 const long long c = level(g, 0).at(i, j);
-                v[0] = __ldcg(P.olf_r + c) * __ldcg(P.olf_w + c);
-            }
+                v[0] += __ldcg(P.olf_r + c) * __ldcg(P.olf_w + c);
+            });
             olf_block_sum<1>(v);
             if (tid == 0) pslot(MP_RZ + (it & 1), k) = v[0];
         });
@@ -767,8 +779,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
                     beta = it == 0 ? 0.0 : v[0] / v[1];
                 }
                 double pq[1] = {0.0};
-                int i, j;
-                if (point_of(ch, g, i, j)) {
+                points0(ch, g, [&](int i, int j) {
                     const Lvl f = level(g, 0);
                     const long long c = f.at(i, j);
                     const OlfCoef cf = olf_coef(P, D, c, ctot);
@@ -778,8 +789,8 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
                     const double q = it == 0 ? az : az + beta * P.olf_s[c];
                     P.olf_p[c] = p;
                     P.olf_s[c] = q;
-                    pq[0] = p * q;
-                }
+                    pq[0] += p * q;
+                });
                 olf_block_sum<1>(pq);
                 if (tid == 0) pslot(MP_PQ, k) = pq[0];
             });
@@ -799,16 +810,15 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
                     alpha = (v[1] > 0.0 && v[0] > 0.0 && v[1] < 1e300) ? v[0] / v[1] : 0.0;
                 }
                 double rr[1] = {0.0};
-                int i, j;
-                if (point_of(ch, g, i, j)) {
+                points0(ch, g, [&](int i, int j) {
                     const long long c = level(g, 0).at(i, j);
                     const OlfCoef cf = olf_coef(P, D, c, ctot);
                     P.H[c] += alpha * P.olf_p[c];
                     const double r = P.olf_r[c] - alpha * P.olf_s[c];
                     P.olf_r[c] = r;
                     P.olf_z[c] = 0.8 / cf.dg * r;
-                    rr[0] = r * r;
-                }
+                    rr[0] += r * r;
+                });
                 olf_block_sum<1>(rr);
                 if (tid == 0) pslot(MP_RR, k) = rr[0];
             });
@@ -867,8 +877,8 @@ void mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::
             if (g.nlev == 0 || (l > 0 && l > g.lc)) continue;
             const int tot = g.m[l] * g.n[l];
             if (l == 0) g.c0_first = (int)chunks.size();
-            for (int f = 0; f < tot; f += OLF_THREADS)
-                chunks.push_back(MgChunk{d, l, f, std::min(OLF_THREADS, tot - f)});
+            const int csize = l == 0 ? MG_CHUNK0 : OLF_THREADS;
+            for (int f = 0; f < tot; f += csize) chunks.push_back(MgChunk{d, l, f, std::min(csize, tot - f)});
             if (l == 0) g.c0_count = (int)chunks.size() - g.c0_first;
         }
     }

@@ -536,13 +536,14 @@ template <typename T, bool DSMEM>
 __device__ __forceinline__ void back_sweep(const ColumnRef &cr, const T *s_d, const T *__restrict__ fc,
                                            T *__restrict__ z) {
     T zn = T(0);
+    const unsigned g0 = (unsigned)cr.g0, sxy = (unsigned)cr.sxy;
     for (int k0 = cr.nz - 1; k0 >= 0; k0 -= BACK_BATCH) {
         T cl[BACK_BATCH], dl[BACK_BATCH];
 #pragma unroll
         for (int q = 0; q < BACK_BATCH; ++q) {
             const int k = k0 - q;
             if (k >= 0) {
-                const long long g = cr.g0 + (long long)k * cr.sxy;
+                const unsigned g = g0 + (unsigned)k * sxy;
                 cl[q] = fc[g];
                 dl[q] = DSMEM ? s_d[k * TILE_THREADS + threadIdx.x] : z[g];
             }
@@ -552,7 +553,7 @@ __device__ __forceinline__ void back_sweep(const ColumnRef &cr, const T *s_d, co
             const int k = k0 - q;
             if (k >= 0) {
                 const T zk = dl[q] - cl[q] * zn;
-                z[cr.g0 + (long long)k * cr.sxy] = zk;
+                z[g0 + (unsigned)k * sxy] = zk;
                 zn = zk;
             }
         }
@@ -801,7 +802,10 @@ __device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_nex
     // the plane above's z and p, the forward sweep's c'_{k-1} and y_{k-1}
     T zc = T(0), pc = T(0), Kc = T(0), fd = T(0), z_up = T(0), p_up = T(0), cprev = T(0), yprev = T(0);
     T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-    long long g = cr.g0;
+    // 32-bit cell offsets (a handle holds fewer than 2^31 cells): fewer live
+    // registers in the sweep than 64-bit indices
+    unsigned g = (unsigned)cr.g0;
+    const unsigned sxy = (unsigned)cr.sxy;
     auto sweep = [&](auto mode) {
         constexpr int MODE = decltype(mode)::value;
         auto zv = [&](const T *zz, const T *tt, int o) {
@@ -872,7 +876,7 @@ __device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_nex
             pc = p_dn;
             Kc = K_dn;
             fd = fu;
-            g += cr.sxy;
+            g += sxy;
         };
         march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next);
     };
