@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--fd-steps", type=int, default=20)
     ap.add_argument("--ensemble-steps", type=int, default=120)
     ap.add_argument("--ensemble-halving-steps", type=int, default=4)
+    ap.add_argument("--schedule-steps", type=int, default=10)
     ap.add_argument("--autotune", type=int, default=1)
     return ap.parse_args()
 
@@ -379,6 +380,34 @@ def run_ensemble(args, local, world=1, rank=0):
     barrier(world)
     ms, launches, diags = ens.run_sharded(doms, nsteps, rank, world, device=local, autotune=2 if args.autotune else 0)
     ms_max = max_over_ranks(ms, world)
+    # the two step schedules on the same first steps: one launch per subsurface
+    # step (fused) and a launch per kernel
+    schedules = {}
+    if world == 1 and args.schedule_steps > 0:
+        import torch
+        import dhara_b200 as db
+        for fused in (1, 0):
+            s = db.Solver([d.params for d in doms], device=local)
+            for i, d in enumerate(doms):
+                s.load(d, i)
+            s.prepare()
+            c = s.launch_config()
+            s.set_launch_config(c["krylov_blocks_per_sm"], c["overland_resident"], c["overland_blocks_per_sm"],
+                                fused_step=fused)
+            stream = torch.cuda.ExternalStream(s.stream, device=local)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            s.synchronize()
+            n0 = s.launch_count()
+            e0.record(stream)
+            s.step(args.schedule_steps, graph=True)
+            e1.record(stream)
+            e1.synchronize()
+            schedules["fused_step" if fused else "launch_per_kernel"] = {
+                "ms_per_step": e0.elapsed_time(e1) / args.schedule_steps,
+                "launches_per_step": (s.launch_count() - n0) / args.schedule_steps}
+            s.close()
+        schedules["steps"] = args.schedule_steps
     worst_mass = 0.0
     kry_nc = olf_nc = solves = 0
     runaway = 0
@@ -405,6 +434,7 @@ def run_ensemble(args, local, world=1, rank=0):
             "picard_steps_at_cap": sum(diags[i]["picard_nonconverged"] for i in range(len(doms))),
             "domain_steps": len(doms) * nsteps,
             "domains_with_abs_psi_above_1e3_m": runaway,
+            "schedules": schedules,
             "note": "the reference's modified Picard iteration diverges on most of these rain-on-dry-soil domains, "
                     "in the oracle exactly as here; the rate measures the path's work, not a physical result"}
 
