@@ -406,6 +406,14 @@ def run_ensemble(args, local, world=1, rank=0):
             schedules["fused_step" if fused else "launch_per_kernel"] = {
                 "ms_per_step": e0.elapsed_time(e1) / args.schedule_steps,
                 "launches_per_step": (s.launch_count() - n0) / args.schedule_steps}
+            if not fused:
+                # where a step's time goes: the same steps again with per-kernel events
+                s.set_kernel_timing(True)
+                s.reset_kernel_timing()
+                s.step(args.schedule_steps)
+                s.synchronize()
+                schedules["kernel_ms_per_step"] = {k: s.kernel_timing(k)[1] / args.schedule_steps
+                                                   for k in db.KERNELS if s.kernel_timing(k)[0]}
             s.close()
         schedules["steps"] = args.schedule_steps
     worst_mass = 0.0
