@@ -257,6 +257,25 @@ def run_ours(args, world, rank, local):
     s2.close()
     ms_h = max_over_ranks(ms_h, world)
     mixed_same_horizon = world * N * min(args.fp64_steps, args.steps) / (ms_h / 1e3)
+    # and with the constitutive closure in FP32 (closure_fp32; its parity
+    # against the oracle is in error_vs_oracle)
+    closure_fp32 = None
+    if args.fp64_steps > 0:
+        q4 = type(p).from_buffer_copy(p)
+        q4.closure_fp32 = 1
+        s4 = db.Solver(q4, device=local)
+        s4.load(dom)
+        s4.prepare()
+        s4.set_launch_config(launch_cfg["krylov_blocks_per_sm"], launch_cfg["overland_resident"],
+                             launch_cfg["overland_blocks_per_sm"], launch_cfg["tile_shape"], launch_cfg["fused_step"])
+        ms_c, _ = timed(s4, min(args.fp64_steps, args.steps))
+        dg4 = s4.diagnostics()
+        s4.close()
+        ms_c = max_over_ranks(ms_c, world)
+        closure_fp32 = {"value": world * N * min(args.fp64_steps, args.steps) / (ms_c / 1e3),
+                        "speedup_vs_fp64": None,
+                        "mass_error_over_inflow": (dg4["storage_change_cum"] - (dg4["top_inflow_cum"] -
+                                                   dg4["bottom_outflow_cum"])) / dg4["top_inflow_cum"]}
 
     # end to end through the public API: per step upload the step's rain field
     # from pinned host memory, advance, read back the ponded depth and the
@@ -338,6 +357,8 @@ def run_ours(args, world, rank, local):
                    "l2": "inputs larger than L2 (~0.8 GB working set per step)",
                    "parallelism": f"replicas x{world}"},
         "fp64_value": fp64_value, "mixed_same_horizon": mixed_same_horizon,
+        "mixed_closure_fp32": (dict(closure_fp32, speedup_vs_fp64=closure_fp32["value"] / fp64_value)
+                               if closure_fp32 and fp64_value else closure_fp32),
         "speedup_mixed_vs_fp64": (mixed_same_horizon / fp64_value) if fp64_value else None,
         "mass_error_over_inflow": mass_err / inflow if inflow else None,
         "picard_iters": dg["picard_iters_total"], "krylov_inner_iters": dg["krylov_iters_total"],
@@ -694,9 +715,10 @@ def error_vs_oracle(args, local, nsteps=8):
            "oracle": "FP64, column-preconditioned CG to 1e-12 relative residual, CG overland",
            "oracle_spread": sh.free_run_drift(d_or, nsteps, oracle.SOLVER_CG, oracle.SOLVER_PCG_COLUMN)}
     fields = ("psi", "theta", "ponding", "waterelev")
-    for name, prec in (("mixed", db.MIXED), ("fp64", db.FP64)):
+    for name, prec, cf32 in (("mixed", db.MIXED, 0), ("fp64", db.FP64, 0), ("mixed_closure_fp32", db.MIXED, 1)):
         p = type(d.params).from_buffer_copy(d.params)
         p.precision = prec
+        p.closure_fp32 = cf32
         dd = inputs.Domain(params=p, fields=d.fields, int_fields=d.int_fields, rain_mm=d.rain_mm)
         g, _, _ = db.run(dd, nsteps=nsteps, device=local)
         s = db.Solver(p, device=local)
