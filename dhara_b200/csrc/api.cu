@@ -721,8 +721,9 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     std::vector<MgChunk> mgc;
     int lchunk[MG_MAXLEV + 2];
     int mg_lg = 0;
-    long long mg_nc = 0;
-    mg_plan(h->hdom, mgd, mgc, lchunk, mg_lg, mg_nc);
+    long long mg_nc = 0, mg_npw = 0, mg_ndinv = 0;
+    if (!mg_plan(h->hdom, mgd, mgc, lchunk, mg_lg, mg_nc, mg_npw, mg_ndinv))
+        return bail(fail(DHARA_ERR_UNSUPPORTED, "a surface grid needs more than %d multigrid levels", MG_MAXLEV));
     MgDom *d_mgd = nullptr;
     MgChunk *d_mgc = nullptr;
     const int nchunk0 = lchunk[1] - lchunk[0];
@@ -730,6 +731,8 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     rc |= dalloc(h, &d_mgc, std::max<size_t>(mgc.size(), 1));
     rc |= dalloc(h, &P.mg_a, 5 * (size_t)std::max(mg_nc, 1LL));
     for (double **q : {&P.mg_w, &P.mg_b, &P.mg_x, &P.mg_t}) rc |= dalloc(h, q, (size_t)std::max(mg_nc, 1LL));
+    rc |= dalloc(h, &P.mg_pw, (size_t)std::max(mg_npw, 1LL));
+    rc |= dalloc(h, &P.mg_dinv, (size_t)std::max(mg_ndinv, 1LL));
     rc |= dalloc(h, &P.mg_part, 5 * (size_t)std::max(nchunk0, 1));
     rc |= dalloc(h, &P.mgctl, ndomains);
     OlfSeg *d_oseg = nullptr;
@@ -803,6 +806,8 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     e = e ? e : zero(P.mg_part, 5 * (size_t)std::max(nchunk0, 1) * 8);
     for (double *q : {P.mg_a, P.mg_w, P.mg_b, P.mg_x, P.mg_t})
         e = e ? e : zero(q, (q == P.mg_a ? 5 : 1) * (size_t)std::max(mg_nc, 1LL) * 8);
+    e = e ? e : zero(P.mg_pw, (size_t)std::max(mg_npw, 1LL) * sizeof(float4));
+    e = e ? e : zero(P.mg_dinv, (size_t)std::max(mg_ndinv, 1LL) * 8);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_mgd, mgd.data(), sizeof(MgDom) * mgd.size(), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess && !mgc.empty())

@@ -36,6 +36,14 @@
 #ifndef STAGES
 #define STAGES 2
 #endif
+// inner sweep: chunks prefetched into L2 beyond the staged ones (0: none).
+// Measured per FP32 / FP64 inner iteration on the 512x512x40 storm: 0 chunks
+// 0.1681 / 0.2595 ms, 1 chunk 0.1644 / 0.2548, 2 chunks 0.1664 / 0.2609,
+// 4 chunks 0.1749 / 0.2868 (prefetching further evicts the neighbour tiles'
+// halo planes from L2 before they are read).
+#ifndef PF_DIST
+#define PF_DIST 1
+#endif
 // Krylov kernel: blocks per SM it is compiled for (register budget), and
 // whether the FP32 column solve keeps its forward-sweep values d' in shared
 // memory (1) or in the t array it then overwrites (0)
@@ -155,20 +163,26 @@ struct OlfSegState {
 // Multigrid hierarchy of the overland solve (overland_mg.cu).  Level 0 is a
 // domain's interior surface grid (the fixed ring eliminated); each coarser
 // level halves every dimension that still has at least 3 points, vertex-
-// centred (coarse point I sits on fine point 2I+1), down to at most 2 x 2.
-#define MG_MAXLEV 16
-#define MG_SMEM_PTS 1536     // a domain's coarsest levels, up to this many points together, run in one block
-#define MG_SMEM_BYTES (MG_SMEM_PTS * 9 * 8)  // their operators, weights and vectors in shared memory
-#define MG_COARSE_SWEEPS 7   // smoothing sweeps on the coarsest level (odd: the result ends in t)
+// centred (coarse point I sits on fine point 2I+1), until a level has at most
+// MG_DENSE_PTS points, which is solved exactly (a dense inverse).
+#define MG_MAXLEV 20
+#define MG_DENSE_PTS 16      // the coarsest level: at most this many points, solved by its inverse
+#define MG_SMEM_PTS 1248     // a domain's coarsest levels, up to this many points together, run in one block
+// their operators (5), smoother weights, vectors b, x, t and interpolation
+// weights (4 floats) per point, and the coarsest level's inverse
+#define MG_SMEM_BYTES ((MG_SMEM_PTS * 11 + MG_DENSE_PTS * MG_DENSE_PTS) * 8)
 #define MG_CHUNK0 (4 * OLF_THREADS)  // points of a level-0 chunk (the CG's vectors), four per thread
 struct MgDom {
     int nlev;                      // levels; 0 when the domain has no interior cell
     int lc;                        // first level run by the domain's block (levels lc .. nlev-1)
     int nx;                        // surface row length (level 0 indexing)
     int c0_first, c0_count;        // the domain's level-0 chunks (CG partial sums)
+    int pad;
     int m[MG_MAXLEV], n[MG_MAXLEV];             // points per level in x and y
     unsigned char hx[MG_MAXLEV], hy[MG_MAXLEV]; // level l+1 halves x (y) of level l
     long long off[MG_MAXLEV];      // level 0: the domain's surface offset; else first coarse point
+    long long pwo[MG_MAXLEV];      // first interpolation-weight slot of level l (l < nlev - 1)
+    long long dio;                 // first entry of the coarsest level's inverse
 };
 // A run of up to OLF_THREADS (level 0: MG_CHUNK0) consecutive points of one
 // level of one domain.
@@ -246,6 +260,8 @@ struct DevPtrs {
     long long mg_nc;     // coarse points of all domains and levels
     double *mg_a;        // [5][mg_nc]: C, E, N, NE, NW of every coarse row
     double *mg_w, *mg_b, *mg_x, *mg_t;  // [mg_nc] 1/smoother weight, rhs, pre- and post-smoothed
+    float4 *mg_pw;       // interpolation weights of every fine point to its (up to) four parents
+    double *mg_dinv;     // the coarsest level's inverse of every domain (row-major, symmetric)
     double *mg_part;     // [5][mg_nchunk0] chunk partials: p.q, r.r, r.z (two slots), b.b
     MgCtrl *mgctl;       // [ndom]
     // faces
@@ -319,8 +335,8 @@ cudaError_t launch_overland_finish(const DevPtrs &P, long long ctot, cudaStream_
 // Multigrid hierarchy of the overland solve for the given domains: per-domain
 // levels, the chunk lists (level by level) and the number of coarse points.
 cudaError_t launch_overland_mg(const DevPtrs &P, const LaunchCfg &L, long long ctot, cudaStream_t s);
-void mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::vector<MgChunk> &chunks,
-             int (&lchunk)[MG_MAXLEV + 2], int &lg, long long &nc);
+bool mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::vector<MgChunk> &chunks,
+             int (&lchunk)[MG_MAXLEV + 2], int &lg, long long &nc, long long &npw, long long &ndinv);
 cudaError_t configure_mg(LaunchCfg &L, int device);
 // Discrete adjoint (adjoint.cu).  Tape of one checkpoint segment, the
 // carried adjoint state and the gradient accumulators; 3D arrays in the

@@ -8,37 +8,51 @@
 // iterations for a 1e-12 relative residual (1,400-2,100 on 256 x 256 storm
 // surfaces, growing with the grid); the reference's 100-iteration cap stops
 // far from the solution.  A V-cycle removes the smooth error that point
-// smoothing cannot: 60-90 iterations on the same systems in a scipy study,
-// nearly independent of the grid size, and about 50 per solve on the
-// 512 x 512 storm surface.
+// smoothing cannot.
 //
 // Hierarchy (per domain, planned on the host by mg_plan): level 0 is the
 // interior of the surface grid (the fixed ring is eliminated, as in the
 // Jacobi solver); level l+1 halves every dimension of level l that has at
-// least 3 points, vertex-centred (coarse point I sits on fine point 2I+1), so
-// the coarsest level has at most 2 x 2 points.  Prolongation P is bilinear
-// (weights 1 and 1/2 per dimension), restriction is P^T, and the coarse
-// operators are the Galerkin products A_{l+1} = P^T A_l P, recomputed for
-// every solve.  They are 9-point; each row stores C, E, N, NE and NW, and a
-// row's W, S, SW and SE are its neighbours' E, N, NE and NW, so every stored
-// operator is symmetric bit for bit.  The smoother is Jacobi with per-row
-// weights w_i = max(a_ii / 0.8, 0.55 sum_j |a_ij|) (weighted Jacobi at 0.8
-// wherever that is safe): 2W - A is then diagonally dominant, every sweep is
-// convergent, and the V(1,1) cycle -- pre-smoothing from zero, coarse
-// correction, post-smoothing, and MG_COARSE_SWEEPS sweeps on the coarsest
-// level -- is a fixed symmetric positive definite operator, as CG needs.
+// least 3 points, vertex-centred (coarse point I sits on fine point 2I+1),
+// until a level has at most MG_DENSE_PTS points; that coarsest level is
+// solved exactly by its inverse, formed once per solve.
+//
+// Interpolation is operator-dependent (the "black box" multigrid rule of
+// Dendy, J. Comput. Phys. 48 (1982) 366-386), because the conductance jumps
+// by orders of magnitude between ponded and dry cells and bilinear
+// interpolation across such a jump is poor: a fine point between two coarse
+// points along x takes weights -sum(column W) / sum(column C) and
+// -sum(column E) / sum(column C) of its row's 3 x 3 stencil (the row collapsed
+// onto the line through the coarse points; along y likewise with the stencil's
+// rows), and a point between four coarse points takes the weights its row
+// gives once its four edge neighbours are replaced by their own
+// interpolation.  The stencils are first made M-matrix rows (positive
+// off-diagonal entries moved onto the diagonal) and every weight is clamped
+// to [0, 1]; weights are stored in FP32 and used, converted, in FP64.  The
+// coarse operators are the Galerkin products A_{l+1} = P^T A_l P with these
+// weights, recomputed for every solve.  They are 9-point; each row stores C,
+// E, N, NE and NW, and a row's W, S, SW and SE are its neighbours' E, N, NE
+// and NW, so every stored operator is symmetric bit for bit.  The smoother is
+// Jacobi with per-row weights w_i = max(a_ii / 0.8, 0.55 sum_j |a_ij|)
+// (weighted Jacobi at 0.8 wherever that is safe): 2W - A is then diagonally
+// dominant, every sweep is convergent, and the V(1,1) cycle -- pre-smoothing
+// from zero, coarse correction, post-smoothing, and the exact solve on the
+// coarsest level (its inverse symmetrised) -- is a fixed symmetric positive
+// definite operator, as CG needs.  On 128 x 128 storm surfaces this takes
+// 39-47 CG iterations where bilinear interpolation took 63-81.
 //
 // Schedule: one persistent cooperative launch per solve for all domains.  A
 // domain's coarsest levels, as many as fit MG_SMEM_PTS points together, run
-// in one block out of shared memory with block barriers; the finer ones run
-// as grid phases, level 0 in chunks of MG_CHUNK0 points (four per thread) and
-// the others one point per thread.  The residual is fused into the
-// restriction and the prolongation into the post-smoothing (each point
-// recomputes the few neighbour values it needs), so a grid level costs one
-// barrier on the way down and one on the way up; with q = A z + beta q the CG
-// forms p and q in one phase.  An iteration with L grid levels is 2 L + 3
-// barriers (eleven on a 512 x 512 surface).  Every reduction runs over chunks
-// in a fixed order, so results do not depend on the block count.
+// in one block out of shared memory with block barriers, their operators set
+// up there and kept for the whole solve when the block owns one domain; the
+// finer ones run as grid phases, level 0 in chunks of MG_CHUNK0 points (four
+// per thread) and the others one point per thread.  The residual is fused
+// into the restriction and the prolongation into the post-smoothing (each
+// point recomputes the few neighbour values it needs), so a grid level costs
+// one barrier on the way down and one on the way up; with q = A z + beta q
+// the CG forms p and q in one phase.  An iteration with L grid levels is
+// 2 L + 3 barriers (eleven on a 512 x 512 surface).  Every reduction runs over
+// chunks in a fixed order, so results do not depend on the block count.
 #include <algorithm>
 #include <cstring>
 
@@ -77,39 +91,16 @@ __device__ __forceinline__ LvlVec vectors(const DevPtrs &P, int l) {
     return LvlVec{P.mg_b, P.mg_x, P.mg_t};
 }
 
-// Parents of fine index i (level l) on level l+1 along one dimension: the
-// coarse point on it (weight 1) or the two beside it (1/2 each, those inside
-// the level); identity where the dimension is not halved.
-__device__ __forceinline__ int parents(int i, bool halves, int mc, int (&I)[2], double (&w)[2]) {
-    if (!halves) {
-        I[0] = i;
-        w[0] = 1.0;
-        return 1;
-    }
-    if (i & 1) {
-        I[0] = (i - 1) >> 1;
-        w[0] = 1.0;
-        return 1;
-    }
-    int k = 0;
-    if (i >= 2) { I[k] = (i >> 1) - 1; w[k] = 0.5; ++k; }
-    if ((i >> 1) < mc) { I[k] = i >> 1; w[k] = 0.5; ++k; }
-    return k;
+// Interpolation weights of level l's point (i, j) to its parents, in the slot
+// order (p0x, p0y), (p1x, p0y), (p0x, p1y), (p1x, p1y) of parents2.
+__device__ __forceinline__ float4 *pw_ptr(const DevPtrs &P, const MgDom &g, int l, int i, int j) {
+    return P.mg_pw + g.pwo[l] + (long long)j * g.m[l] + i;
 }
-
-// Children of coarse index I (level l+1) on level l along one dimension:
-// 2I, 2I+1, 2I+2 with weights 1/2, 1, 1/2 (those inside the level).
-__device__ __forceinline__ int children(int I, bool halves, int mf, int (&f)[3], double (&w)[3]) {
-    if (!halves) {
-        f[0] = I;
-        w[0] = 1.0;
-        return 1;
-    }
-    int k = 0;
-    f[k] = 2 * I; w[k] = 0.5; ++k;
-    f[k] = 2 * I + 1; w[k] = 1.0; ++k;
-    if (2 * I + 2 < mf) { f[k] = 2 * I + 2; w[k] = 0.5; ++k; }
-    return k;
+__device__ __forceinline__ float4 pw_at(const DevPtrs &P, const MgDom &g, int l, int i, int j) {
+    return __ldcg(pw_ptr(P, g, l, i, j));
+}
+__device__ __forceinline__ double slot(const float4 &w, int s) {
+    return (double)(s == 0 ? w.x : s == 1 ? w.y : s == 2 ? w.z : w.w);
 }
 
 // Row (i, j) of level l's operator as a 3 x 3 stencil a[dj+1][di+1]; zero
@@ -215,63 +206,25 @@ __device__ __forceinline__ double smoother_inv(const Row9 &r) {
     return 1.0 / fmax(r.a[1][1] / 0.8, 0.55 * l1);
 }
 
-// ---------------------------------------------------------- point kernels
-// Galerkin row (I, J) of level l+1: C, E, N, NE and NW of P^T A_l P.
-__device__ void galerkin_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l,
-                               int I, int J) {
-    const Lvl f = level(g, l), c = level(g, l + 1);
-    const bool hx = g.hx[l], hy = g.hy[l];
-    int fx[3], fy[3];
-    double wx[3], wy[3];
-    const int nfx = children(I, hx, f.m, fx, wx), nfy = children(J, hy, f.n, fy, wy);
-    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int b = 0; b < nfy; ++b)
-        for (int a = 0; a < nfx; ++a) {
-            const double wf = wx[a] * wy[b];
-            const Row9 r = row_of(P, D, ctot, g, l, f, fx[a], fy[b]);
-            for (int dy = -1; dy <= 1; ++dy)
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const double av = r.a[dy + 1][dx + 1];
-                    if (av == 0.0) continue;
-                    int px[2], py[2];
-                    double ux[2], uy[2];
-                    const int npx = parents(fx[a] + dx, hx, c.m, px, ux);
-                    const int npy = parents(fy[b] + dy, hy, c.n, py, uy);
-                    for (int q = 0; q < npy; ++q)
-                        for (int p = 0; p < npx; ++p) {
-                            const int di = px[p] - I, dj = py[q] - J;
-                            const int k = (di == 0 && dj == 0) ? 0 : (di == 1 && dj == 0) ? 1
-                                        : (di == 0 && dj == 1)   ? 2 : (di == 1 && dj == 1) ? 3
-                                        : (di == -1 && dj == 1)  ? 4 : -1;
-                            if (k >= 0) acc[k] += wf * av * ux[p] * uy[q];
-                        }
-                }
-        }
-    const long long at = c.at(I, J);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) P.mg_a[(size_t)k * P.mg_nc + at] = acc[k];
-}
-
-__device__ __forceinline__ void weight_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g,
-                                             int l, int i, int j) {
-    const Lvl v = level(g, l);
-    P.mg_w[v.at(i, j)] = smoother_inv(row_of(P, D, ctot, g, l, v, i, j));
-}
-
+// ---------------------------------------------------- transfer operators
 // Child a (0, 1, 2 = 2I, 2I+1, 2I+2) of coarse index I along a halved
-// dimension, or I itself (a = 1) along one that is not; weight 0 for none.
+// dimension, or I itself (a = 1) along one that is not; w = 0 for none.
 __device__ __forceinline__ void child(int I, int a, bool halves, int mf, int &f, double &w) {
     if (halves) {
         f = 2 * I + a;
-        w = f < mf ? (a == 1 ? 1.0 : 0.5) : 0.0;
+        w = f < mf ? 1.0 : 0.0;
     } else {
         f = I;
         w = a == 1 ? 1.0 : 0.0;
     }
 }
 
-// Parents p0, p1 of fine index i along one dimension with weights u0, u1 (0
-// for none): the coarse point on i, or the two beside it.
+// The weight slot of child a's parent I along one dimension: the child 2I
+// has I as its second parent, 2I+1 and 2I+2 as their first.
+__device__ __forceinline__ int child_slot(int a, bool halves) { return (halves && a == 0) ? 1 : 0; }
+
+// Parents p0, p1 of fine index i along one dimension with u0, u1 nonzero
+// where the parent exists: the coarse point on i, or the two beside it.
 __device__ __forceinline__ void parents2(int i, bool halves, int mc, int &p0, double &u0, int &p1, double &u1) {
     if (!halves) {
         p0 = p1 = i;
@@ -286,21 +239,175 @@ __device__ __forceinline__ void parents2(int i, bool halves, int mc, int &p0, do
         u0 = p0 >= 0 ? 0.5 : 0.0;
         p1 = i >> 1;
         u1 = p1 < mc ? 0.5 : 0.0;
-        p0 = p0 < 0 ? 0 : p0;  // a parent of weight 0 points at a valid slot
+        p0 = p0 < 0 ? 0 : p0;  // a parent that does not exist points at a valid slot
         p1 = p1 < mc ? p1 : mc - 1;
     }
 }
 
-// (P t)(i, j): level l+1's t interpolated to level l's point (i, j).
-__device__ __forceinline__ double prolong_at(const MgDom &g, int l, const Lvl &c, const double *tc, int i, int j) {
+__device__ __forceinline__ double clamp01(double v) { return v > 0.0 ? (v < 1.0 ? v : 1.0) : 0.0; }
+
+// The row with its positive off-diagonal entries moved onto the diagonal.
+__device__ __forceinline__ Row9 lumped(Row9 r) {
+    double add = 0.0;
+#pragma unroll
+    for (int y = 0; y < 3; ++y)
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+            if ((y != 1 || x != 1) && r.a[y][x] > 0.0) {
+                add += r.a[y][x];
+                r.a[y][x] = 0.0;
+            }
+    r.a[1][1] += add;
+    return r;
+}
+
+struct W4 {
+    double w[4];
+};
+
+// Weights of a point between two coarse points: along x (ex) the stencil's
+// columns are summed, along y its rows.
+__device__ __forceinline__ W4 edge_weights(const Row9 &s, bool ex) {
+    W4 o = {{0.0, 0.0, 0.0, 0.0}};
+    if (ex) {
+        const double cC = (s.a[0][1] + s.a[1][1]) + s.a[2][1];
+        if (cC > 0.0) {
+            o.w[0] = clamp01(-((s.a[0][0] + s.a[1][0]) + s.a[2][0]) / cC);
+            o.w[1] = clamp01(-((s.a[0][2] + s.a[1][2]) + s.a[2][2]) / cC);
+        }
+    } else {
+        const double cC = (s.a[1][0] + s.a[1][1]) + s.a[1][2];
+        if (cC > 0.0) {
+            o.w[0] = clamp01(-((s.a[0][0] + s.a[0][1]) + s.a[0][2]) / cC);
+            o.w[2] = clamp01(-((s.a[2][0] + s.a[2][1]) + s.a[2][2]) / cC);
+        }
+    }
+    return o;
+}
+
+// Interpolation weights of point (i, j) of an m x n level (rowf(i, j): the
+// level's rows, only called inside the level).
+template <typename RowF>
+__device__ __forceinline__ float4 interp_weights(RowF rowf, int i, int j, int m, int n, bool hx, bool hy) {
+    const bool ex = hx && !(i & 1), ey = hy && !(j & 1);
+    if (!ex && !ey) return make_float4(1.f, 0.f, 0.f, 0.f);
+    const Row9 s = lumped(rowf(i, j));
+    W4 o = {{0.0, 0.0, 0.0, 0.0}};
+    if (!(ex && ey)) {
+        o = edge_weights(s, ex);
+    } else if (s.a[1][1] > 0.0) {
+        double acc[4] = {s.a[0][0], s.a[0][2], s.a[2][0], s.a[2][2]};
+        if (i > 0) {
+            const W4 e = edge_weights(lumped(rowf(i - 1, j)), false);
+            acc[0] += s.a[1][0] * e.w[0];
+            acc[2] += s.a[1][0] * e.w[2];
+        }
+        if (i < m - 1) {
+            const W4 e = edge_weights(lumped(rowf(i + 1, j)), false);
+            acc[1] += s.a[1][2] * e.w[0];
+            acc[3] += s.a[1][2] * e.w[2];
+        }
+        if (j > 0) {
+            const W4 e = edge_weights(lumped(rowf(i, j - 1)), true);
+            acc[0] += s.a[0][1] * e.w[0];
+            acc[1] += s.a[0][1] * e.w[1];
+        }
+        if (j < n - 1) {
+            const W4 e = edge_weights(lumped(rowf(i, j + 1)), true);
+            acc[2] += s.a[2][1] * e.w[0];
+            acc[3] += s.a[2][1] * e.w[1];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) o.w[k] = clamp01(-acc[k] / s.a[1][1]);
+    }
+    return make_float4((float)o.w[0], (float)o.w[1], (float)o.w[2], (float)o.w[3]);
+}
+
+// Galerkin row (I, J) of the coarse level: C, E, N, NE and NW of P^T A P, from
+// the fine level's rows rowf and weights wf (fm x fn fine points, cm x cn
+// coarse).
+template <typename RowF, typename WF>
+__device__ __forceinline__ void galerkin_row(RowF rowf, WF wf, int fm, int fn, bool hx, bool hy, int cm, int cn,
+                                             int I, int J, double (&acc)[5]) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) acc[k] = 0.0;
+    for (int b = 0; b < 3; ++b) {
+        int fy;
+        double vy;
+        child(J, b, hy, fn, fy, vy);
+        if (vy == 0.0) continue;
+        for (int a = 0; a < 3; ++a) {
+            int fx;
+            double vx;
+            child(I, a, hx, fm, fx, vx);
+            if (vx == 0.0) continue;
+            const double pf = slot(wf(fx, fy), child_slot(a, hx) + 2 * child_slot(b, hy));
+            if (pf == 0.0) continue;
+            const Row9 r = rowf(fx, fy);
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const double av = r.a[dy + 1][dx + 1];
+                    if (av == 0.0) continue;
+                    const int gx = fx + dx, gy = fy + dy;
+                    const float4 wg = wf(gx, gy);
+                    int px0, px1, py0, py1;
+                    double ux0, ux1, uy0, uy1;
+                    parents2(gx, hx, cm, px0, ux0, px1, ux1);
+                    parents2(gy, hy, cn, py0, uy0, py1, uy1);
+                    for (int s = 0; s < 4; ++s) {
+                        const double w = slot(wg, s);
+                        const double u = ((s & 1) ? ux1 : ux0) * ((s & 2) ? uy1 : uy0);
+                        if (w == 0.0 || u == 0.0) continue;
+                        const int di = ((s & 1) ? px1 : px0) - I, dj = ((s & 2) ? py1 : py0) - J;
+                        const int k = (di == 0 && dj == 0) ? 0 : (di == 1 && dj == 0) ? 1
+                                    : (di == 0 && dj == 1)   ? 2 : (di == 1 && dj == 1) ? 3
+                                    : (di == -1 && dj == 1)  ? 4 : -1;
+                        if (k >= 0) acc[k] += (pf * av) * w;
+                    }
+                }
+        }
+    }
+}
+
+// ------------------------------------------------- grid-phase point kernels
+// Galerkin row (I, J) of level l+1 from level l in global memory.
+__device__ void galerkin_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l,
+                               int I, int J) {
+    const Lvl f = level(g, l), c = level(g, l + 1);
+    double acc[5];
+    galerkin_row([&](int i, int j) { return row_of(P, D, ctot, g, l, f, i, j); },
+                 [&](int i, int j) { return pw_at(P, g, l, i, j); }, f.m, f.n, g.hx[l], g.hy[l], c.m, c.n, I, J,
+                 acc);
+    const long long at = c.at(I, J);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) P.mg_a[(size_t)k * P.mg_nc + at] = acc[k];
+}
+
+// Smoother weight (levels >= 1) and interpolation weights of level l's point.
+__device__ __forceinline__ void weight_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g,
+                                             int l, int i, int j) {
+    const Lvl v = level(g, l);
+    auto rowf = [&](int ii, int jj) { return row_of(P, D, ctot, g, l, v, ii, jj); };
+    if (l > 0) P.mg_w[v.at(i, j)] = smoother_inv(rowf(i, j));
+    *pw_ptr(P, g, l, i, j) = interp_weights(rowf, i, j, v.m, v.n, g.hx[l], g.hy[l]);
+}
+
+// (P t)(i, j): level l+1's t interpolated to level l's point (i, j) with the
+// point's weights w.
+__device__ __forceinline__ double prolong_at(const MgDom &g, int l, const Lvl &c, const double *tc, const float4 &w,
+                                             int i, int j) {
     int px0, px1, py0, py1;
     double ux0, ux1, uy0, uy1;
     parents2(i, g.hx[l], c.m, px0, ux0, px1, ux1);
     parents2(j, g.hy[l], c.n, py0, uy0, py1, uy1);
-    // every parent slot is valid (weight 0 where there is no parent), so the
-    // four loads are unconditional
-    return (ux0 * uy0 * __ldcg(tc + c.at(px0, py0)) + ux1 * uy0 * __ldcg(tc + c.at(px1, py0))) +
-           (ux0 * uy1 * __ldcg(tc + c.at(px0, py1)) + ux1 * uy1 * __ldcg(tc + c.at(px1, py1)));
+    // every parent slot is valid (a weight that does not apply is selected
+    // to 0), so the four loads are unconditional
+    const double w00 = (ux0 != 0.0 && uy0 != 0.0) ? (double)w.x : 0.0;
+    const double w10 = (ux1 != 0.0 && uy0 != 0.0) ? (double)w.y : 0.0;
+    const double w01 = (ux0 != 0.0 && uy1 != 0.0) ? (double)w.z : 0.0;
+    const double w11 = (ux1 != 0.0 && uy1 != 0.0) ? (double)w.w : 0.0;
+    return (w00 * __ldcg(tc + c.at(px0, py0)) + w10 * __ldcg(tc + c.at(px1, py0))) +
+           (w01 * __ldcg(tc + c.at(px0, py1)) + w11 * __ldcg(tc + c.at(px1, py1)));
 }
 
 // Grid levels (one barrier per level each way): level l+1 point (I, J) gets
@@ -312,19 +419,22 @@ __device__ void restrict_point(const DevPtrs &P, const DomainDesc &D, long long 
                                int J) {
     const Lvl f = level(g, l), c = level(g, l + 1);
     const LvlVec vf = vectors(P, l);
+    const bool hx = g.hx[l], hy = g.hy[l];
     double acc = 0.0;
 #pragma unroll
     for (int b = 0; b < 3; ++b)
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             int fx, fy;
-            double wx, wy;
-            child(I, a, g.hx[l], f.m, fx, wx);
-            child(J, b, g.hy[l], f.n, fy, wy);
+            double vx, vy;
+            child(I, a, hx, f.m, fx, vx);
+            child(J, b, hy, f.n, fy, vy);
             fx = clampi(fx, f.m);
             fy = clampi(fy, f.n);
+            const float4 wv = pw_at(P, g, l, fx, fy);
+            const double pf = (vx != 0.0 && vy != 0.0) ? slot(wv, child_slot(a, hx) + 2 * child_slot(b, hy)) : 0.0;
             const Row9 r = row_nb<FINE>(P, D, ctot, f, fx, fy);
-            acc += (wx * wy) * (__ldcg(vf.b + f.at(fx, fy)) - apply_nb<FINE>(r, vf.x, f, fx, fy));
+            acc += pf * (__ldcg(vf.b + f.at(fx, fy)) - apply_nb<FINE>(r, vf.x, f, fx, fy));
         }
     const long long at = c.at(I, J);
     P.mg_b[at] = acc;
@@ -347,7 +457,8 @@ __device__ void smooth_up_point(const DevPtrs &P, const DomainDesc &D, long long
         for (int dx = -1; dx <= 1; ++dx) {
             if (FINE && dx != 0 && dy != 0) continue;  // compile-time: no corners at level 0
             const int ni = clampi(i + dx, f.m), nj = clampi(j + dy, f.n);
-            const double xp = __ldcg(vf.x + f.at(ni, nj)) + prolong_at(g, l, c, P.mg_t, ni, nj);
+            const double xp =
+                __ldcg(vf.x + f.at(ni, nj)) + prolong_at(g, l, c, P.mg_t, pw_at(P, g, l, ni, nj), ni, nj);
             ax += r.a[dy + 1][dx + 1] * xp;
             if (dx == 0 && dy == 0) xc = xp;
         }
@@ -357,35 +468,16 @@ __device__ void smooth_up_point(const DevPtrs &P, const DomainDesc &D, long long
 }
 
 // ----------------------------------------------------------- block levels
-// Runs fn(i, j) over every point of level l of the domain with this block.
-template <typename Fn>
-__device__ __forceinline__ void block_points(const MgDom &g, int l, Fn fn) {
-    const int m = g.m[l], tot = m * g.n[l];
-    for (int p = threadIdx.x; p < tot; p += blockDim.x) fn(p % m, p / m);
-}
-
-// The domain's block levels of the set-up: smoother weights of level lc (when
-// lc >= 1; level 0's are formed on the fly), then each coarser operator and
-// its weights.
-__device__ void block_setup(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g) {
-    if (g.lc >= 1) block_points(g, g.lc, [&](int i, int j) { weight_point(P, D, ctot, g, g.lc, i, j); });
-    for (int l = g.lc; l + 1 < g.nlev; ++l) {
-        __syncthreads();
-        block_points(g, l + 1, [&](int i, int j) { galerkin_point(P, D, ctot, g, l, i, j); });
-        __syncthreads();
-        block_points(g, l + 1, [&](int i, int j) { weight_point(P, D, ctot, g, l + 1, i, j); });
-    }
-}
-
-// The domain's block levels of a V-cycle run in shared memory: each level's
-// stored operator (C, E, N, NE, NW; level 0 as the same five from its
-// 5-point rows), smoother weights and vectors b, x, t, levels packed one after
-// another (the host picks lc so that levels lc .. nlev-1 fit MG_SMEM_PTS).
-// Loaded once per cycle; from x_lc = W^-1 b_lc (already formed) down to the
-// coarsest level, its sweeps, and back up; level lc's result goes back to its
-// t vector in global memory.
+// A domain's block levels live in shared memory: each level's operator (C, E,
+// N, NE, NW; level 0 as the same five from its 5-point rows), smoother
+// weights, vectors b, x, t and interpolation weights, levels packed one after
+// another (the host picks lc so that levels lc .. nlev-1 fit MG_SMEM_PTS), and
+// the coarsest level's inverse.  The block sets them up once per solve and
+// keeps them while it owns one domain; a block that owns several reloads a
+// domain's from global memory before its V-cycle.
 struct SmemMG {
-    double *a[5], *w, *b, *x, *t;
+    double *a[5], *w, *b, *x, *t, *dinv;
+    float4 *pw;
 };
 
 __device__ __forceinline__ SmemMG smem_mg(double *base) {
@@ -396,6 +488,8 @@ __device__ __forceinline__ SmemMG smem_mg(double *base) {
     S.b = base + 6 * (size_t)MG_SMEM_PTS;
     S.x = base + 7 * (size_t)MG_SMEM_PTS;
     S.t = base + 8 * (size_t)MG_SMEM_PTS;
+    S.pw = (float4 *)(base + 9 * (size_t)MG_SMEM_PTS);
+    S.dinv = base + 11 * (size_t)MG_SMEM_PTS;
     return S;
 }
 
@@ -437,16 +531,22 @@ __device__ __forceinline__ void s_points(const SL &v, Fn fn) {
     for (int p = threadIdx.x; p < tot; p += blockDim.x) fn(p % v.m, p / v.m);
 }
 
-__device__ void block_vcycle(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, double *smem) {
-    const SmemMG S = smem_mg(smem);
-    SL lv[MG_MAXLEV];
+// Levels lc .. nlev-1 packed in shared memory.
+__device__ __forceinline__ void s_levels(const MgDom &g, SL (&lv)[MG_MAXLEV]) {
     int o = 0;
     for (int l = g.lc; l < g.nlev; ++l) {
         lv[l] = SL{g.m[l], g.n[l], o};
         o += g.m[l] * g.n[l];
     }
-    // ---- load the operators, weights and the top level's b and x
-    for (int l = g.lc; l < g.nlev; ++l) {
+}
+
+// Level lc's operator into shared memory (level 0: from the conductances)
+// with, when `all`, the coarser operators, the smoother and interpolation
+// weights and the coarsest inverse that the set-up left in global memory.
+__device__ void block_load(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, const SmemMG &S,
+                           const SL (&lv)[MG_MAXLEV], bool all) {
+    const int last = all ? g.nlev - 1 : g.lc;
+    for (int l = g.lc; l <= last; ++l) {
         const SL v = lv[l];
         const Lvl gl = level(g, l);
         s_points(v, [&](int i, int j) {
@@ -459,22 +559,133 @@ __device__ void block_vcycle(const DevPtrs &P, const DomainDesc &D, long long ct
                 S.a[2][q] = -cf.cn;
                 S.a[3][q] = 0.0;
                 S.a[4][q] = 0.0;
-                S.w[q] = 0.8 / cf.dg;
             } else {
 #pragma unroll
                 for (int k = 0; k < 5; ++k) S.a[k][q] = __ldcg(P.mg_a + (size_t)k * P.mg_nc + at);
-                S.w[q] = __ldcg(P.mg_w + at);
             }
-            if (l == g.lc) {
-                const LvlVec gv = vectors(P, l);
-                S.b[q] = __ldcg(gv.b + at);
-                S.x[q] = __ldcg(gv.x + at);
+            if (all && l + 1 < g.nlev) {
+                S.w[q] = l == 0 ? 0.8 / S.a[0][q] : __ldcg(P.mg_w + at);
+                S.pw[q] = pw_at(P, g, l, i, j);
             }
         });
     }
-    // ---- down
+    if (all) {
+        const int nd = g.m[g.nlev - 1] * g.n[g.nlev - 1];
+        for (int k = threadIdx.x; k < nd * nd; k += blockDim.x) S.dinv[k] = __ldcg(P.mg_dinv + g.dio + k);
+    }
+}
+
+// Inverse of the coarsest level's operator (at most MG_DENSE_PTS points) by
+// Gauss-Jordan elimination on [A | I] in the scratch M, one warp, lane c
+// owning column c; the result is symmetrised and written to S.dinv and dst.
+// No pivoting: the operator is symmetric positive definite.
+__device__ void dense_inverse(const SmemMG &S, const SL &v, double *M, double *dst) {
+    constexpr int W = 2 * MG_DENSE_PTS;
+    const int n = v.m * v.n, lane = threadIdx.x;
+    if (lane < 2 * n)
+        for (int r = 0; r < n; ++r) {
+            double val = 0.0;
+            if (lane < n) {
+                const int ri = r % v.m, rj = r / v.m, ci = lane % v.m, cj = lane / v.m;
+                const int dx = ci - ri, dy = cj - rj;
+                if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1) val = s_row(S, v, ri, rj).a[dy + 1][dx + 1];
+            } else {
+                val = lane - n == r ? 1.0 : 0.0;
+            }
+            M[r * W + lane] = val;
+        }
+    __syncwarp();
+    for (int k = 0; k < n; ++k) {
+        // column k is only read in this step, and its owner writes nothing
+        const double piv = M[k * W + k];
+        if (lane < 2 * n && lane != k) {
+            const double rk = M[k * W + lane] / piv;
+            M[k * W + lane] = rk;
+            for (int r = 0; r < n; ++r)
+                if (r != k) M[r * W + lane] -= M[r * W + k] * rk;
+        }
+        __syncwarp();
+    }
+    for (int e = lane; e < n * n; e += 32) {
+        const int r = e / n, c = e % n;
+        const double s = 0.5 * (M[r * W + n + c] + M[c * W + n + r]);
+        S.dinv[e] = s;
+        dst[e] = s;
+    }
+}
+
+// The domain's block levels of the set-up: for l = lc .. nlev-2 the smoother
+// and interpolation weights of level l and the Galerkin operator of level
+// l+1, then the coarsest level's inverse; in shared memory, and copied to
+// global memory for a block that must reload them.
+__device__ void block_setup(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, double *smem) {
+    const SmemMG S = smem_mg(smem);
+    SL lv[MG_MAXLEV];
+    s_levels(g, lv);
+    block_load(P, D, ctot, g, S, lv, false);
     for (int l = g.lc; l + 1 < g.nlev; ++l) {
         const SL f = lv[l], c = lv[l + 1];
+        const Lvl gf = level(g, l), gc = level(g, l + 1);
+        const bool hx = g.hx[l], hy = g.hy[l];
+        __syncthreads();
+        s_points(f, [&](int i, int j) {
+            const int q = f.at(i, j);
+            const double w = l == 0 ? 0.8 / S.a[0][q] : smoother_inv(s_row(S, f, i, j));
+            S.w[q] = w;
+            if (l > 0) P.mg_w[gf.at(i, j)] = w;
+            const float4 pw = interp_weights([&](int ii, int jj) { return s_row(S, f, ii, jj); }, i, j, f.m, f.n, hx, hy);
+            S.pw[q] = pw;
+            *pw_ptr(P, g, l, i, j) = pw;
+        });
+        __syncthreads();
+        s_points(c, [&](int I, int J) {
+            double acc[5];
+            galerkin_row([&](int i, int j) { return s_row(S, f, i, j); }, [&](int i, int j) { return S.pw[f.at(i, j)]; },
+                         f.m, f.n, hx, hy, c.m, c.n, I, J, acc);
+            const int q = c.at(I, J);
+            const long long at = gc.at(I, J);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                S.a[k][q] = acc[k];
+                P.mg_a[(size_t)k * P.mg_nc + at] = acc[k];
+            }
+        });
+    }
+    __syncthreads();
+    // the vectors' space is free during the set-up: the elimination's scratch
+    if (threadIdx.x < 32) dense_inverse(S, lv[g.nlev - 1], S.x, P.mg_dinv + g.dio);
+    __syncthreads();
+}
+
+// One V-cycle over the block levels: from x_lc = W^-1 b_lc (already formed)
+// down to the coarsest level, its exact solve, and back up; level lc's result
+// goes back to its t vector in global memory.  `resident` is the domain whose
+// set-up is in shared memory.
+__device__ void block_vcycle(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int dom,
+                             double *smem, int &resident) {
+    const SmemMG S = smem_mg(smem);
+    SL lv[MG_MAXLEV];
+    s_levels(g, lv);
+    const bool reload = resident != dom;
+    __syncthreads();  // every thread has read `resident`
+    if (reload) {
+        block_load(P, D, ctot, g, S, lv, true);
+        if (threadIdx.x == 0) resident = dom;
+    }
+    {
+        const SL v = lv[g.lc];
+        const Lvl gl = level(g, g.lc);
+        const LvlVec gv = vectors(P, g.lc);
+        s_points(v, [&](int i, int j) {
+            S.b[v.at(i, j)] = __ldcg(gv.b + gl.at(i, j));
+            S.x[v.at(i, j)] = __ldcg(gv.x + gl.at(i, j));
+        });
+    }
+    const int L = g.nlev - 1;
+    // ---- down
+    for (int l = g.lc; l < L; ++l) {
+        const SL f = lv[l], c = lv[l + 1];
+        const bool hx = g.hx[l], hy = g.hy[l];
         __syncthreads();
         s_points(f, [&](int i, int j) { S.t[f.at(i, j)] = S.b[f.at(i, j)] - s_apply(s_row(S, f, i, j), S.x, f, i, j); });
         __syncthreads();
@@ -485,42 +696,44 @@ __device__ void block_vcycle(const DevPtrs &P, const DomainDesc &D, long long ct
 #pragma unroll
                 for (int aa = 0; aa < 3; ++aa) {
                     int fx, fy;
-                    double wx, wy;
-                    child(I, aa, g.hx[l], f.m, fx, wx);
-                    child(J, bb, g.hy[l], f.n, fy, wy);
-                    if (wx != 0.0 && wy != 0.0) acc += wx * wy * S.t[f.at(fx, fy)];
+                    double vx, vy;
+                    child(I, aa, hx, f.m, fx, vx);
+                    child(J, bb, hy, f.n, fy, vy);
+                    if (vx != 0.0 && vy != 0.0)
+                        acc += slot(S.pw[f.at(fx, fy)], child_slot(aa, hx) + 2 * child_slot(bb, hy)) * S.t[f.at(fx, fy)];
                 }
             const int q = c.at(I, J);
             S.b[q] = acc;
-            S.x[q] = S.w[q] * acc;
+            if (l + 1 < L) S.x[q] = S.w[q] * acc;
         });
     }
-    // ---- coarsest level: MG_COARSE_SWEEPS (odd) sweeps, the result in t
-    const int L = g.nlev - 1;
-    for (int sw = 0; sw < MG_COARSE_SWEEPS; ++sw) {
+    // ---- coarsest level: t = A^-1 b
+    {
         __syncthreads();
-        const double *from = (sw & 1) ? S.t : S.x;
-        double *to = (sw & 1) ? S.x : S.t;
         const SL v = lv[L];
-        s_points(v, [&](int i, int j) {
-            const int q = v.at(i, j);
-            to[q] = from[q] + S.w[q] * (S.b[q] - s_apply(s_row(S, v, i, j), from, v, i, j));
-        });
+        const int nd = v.m * v.n;
+        for (int r = threadIdx.x; r < nd; r += blockDim.x) {
+            double s = 0.0;
+            for (int k = 0; k < nd; ++k) s += S.dinv[r * nd + k] * S.b[v.o + k];
+            S.t[v.o + r] = s;
+        }
     }
     // ---- up: x_l += P t_{l+1}, then t_l = x_l + W^-1 (b_l - A_l x_l)
     for (int l = L - 1; l >= g.lc; --l) {
         const SL f = lv[l], c = lv[l + 1];
+        const bool hx = g.hx[l], hy = g.hy[l];
         __syncthreads();
         s_points(f, [&](int i, int j) {
             int px0, px1, py0, py1;
             double ux0, ux1, uy0, uy1;
-            parents2(i, g.hx[l], c.m, px0, ux0, px1, ux1);
-            parents2(j, g.hy[l], c.n, py0, uy0, py1, uy1);
+            parents2(i, hx, c.m, px0, ux0, px1, ux1);
+            parents2(j, hy, c.n, py0, uy0, py1, uy1);
+            const float4 w = S.pw[f.at(i, j)];
             double sum = 0.0;
-            if (ux0 != 0.0 && uy0 != 0.0) sum += ux0 * uy0 * S.t[c.at(px0, py0)];
-            if (ux1 != 0.0 && uy0 != 0.0) sum += ux1 * uy0 * S.t[c.at(px1, py0)];
-            if (ux0 != 0.0 && uy1 != 0.0) sum += ux0 * uy1 * S.t[c.at(px0, py1)];
-            if (ux1 != 0.0 && uy1 != 0.0) sum += ux1 * uy1 * S.t[c.at(px1, py1)];
+            if (ux0 != 0.0 && uy0 != 0.0) sum += (double)w.x * S.t[c.at(px0, py0)];
+            if (ux1 != 0.0 && uy0 != 0.0) sum += (double)w.y * S.t[c.at(px1, py0)];
+            if (ux0 != 0.0 && uy1 != 0.0) sum += (double)w.z * S.t[c.at(px0, py1)];
+            if (ux1 != 0.0 && uy1 != 0.0) sum += (double)w.w * S.t[c.at(px1, py1)];
             S.x[f.at(i, j)] += sum;
         });
         __syncthreads();
@@ -587,7 +800,9 @@ __device__ __forceinline__ DomSums decision_sums(const DevPtrs &P, const MgDom &
 // --------------------------------------------------------------- the solve
 __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long ctot) {
     extern __shared__ double s_mg[];  // a domain's block levels (block_vcycle)
+    __shared__ int s_resident;        // the domain whose block levels are set up in s_mg
     const int tid = threadIdx.x;
+    if (tid == 0) s_resident = -1;
     // barrier: one counter that every block adds to once per phase (zeroed by
     // k_olf_setup before every solve)
     unsigned int epoch = 0;
@@ -623,7 +838,8 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
     };
     auto active = [&](int d) { return __ldcg(&P.mgctl[d].active) != 0; };
 
-    // ---- S0: r = b - A x, b.b and r.r partials, z = W^-1 r; level-1 operators
+    // ---- S0: r = b - A x, b.b and r.r partials, z = W^-1 r; level 0's
+    // interpolation weights where level 0 is a grid level
     if (blockIdx.x == 0)
         for (int d = tid; d < P.ndom; d += blockDim.x) {
             P.mgctl[d].active = (P.mgd[d].nlev > 0 && !P.dom[d].frozen) ? 1 : 0;
@@ -645,6 +861,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             P.olf_z[c] = 0.8 / cf.dg * r;
             v[0] += r * r;
             v[1] += b * b;
+            if (g.lc >= 1) weight_point(P, D, ctot, g, 0, i, j);
         });
         olf_block_sum<2>(v);
         if (tid == 0) {
@@ -652,28 +869,30 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             pslot(MP_BB, k) = v[1];
         }
     });
-    if (Lg >= 1)
-        chunks(1, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
-            int I, J;
-            if (point_of(ch, g, I, J)) galerkin_point(P, D, ctot, g, 0, I, J);
-        });
     if (!sync()) return;
-    // ---- set-up of the grid levels: A_l and the weights of level l-1
-    for (int l = 2; l <= Lg; ++l) {
+    // ---- set-up of the grid levels: A_l, then level l's smoother and
+    // interpolation weights where level l is a grid level
+    for (int l = 1; l <= Lg; ++l) {
         chunks(l, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
             int I, J;
             if (point_of(ch, g, I, J)) galerkin_point(P, D, ctot, g, l - 1, I, J);
         });
-        chunks(l - 1, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
-            int i, j;
-            if (ch.lev < g.lc && point_of(ch, g, i, j)) weight_point(P, D, ctot, g, l - 1, i, j);
-        });
         if (!sync()) return;
+        if (l < Lg) {
+            chunks(l, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
+                int i, j;
+                if (l < g.lc && point_of(ch, g, i, j)) weight_point(P, D, ctot, g, l, i, j);
+            });
+            if (!sync()) return;
+        }
     }
     // ---- set-up of every domain's block levels
     for (int d = blockIdx.x; d < P.ndom; d += gridDim.x) {
         const MgDom &g = P.mgd[d];
-        if (g.nlev > 0) block_setup(P, P.dom[d], ctot, g);
+        if (g.nlev > 0) {
+            block_setup(P, P.dom[d], ctot, g, s_mg);
+            if (tid == 0) s_resident = d;
+        }
     }
     if (!sync()) return;
 
@@ -738,7 +957,7 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             for (int d = blockIdx.x; d < P.ndom; d += gridDim.x) {
                 const MgDom &g = P.mgd[d];
                 const bool go = Lg == 0 ? live_after(d, it, cd, cl) : active(d);
-                if (go && g.nlev > 0) block_vcycle(P, P.dom[d], ctot, g, s_mg);
+                if (go && g.nlev > 0) block_vcycle(P, P.dom[d], ctot, g, d, s_mg, s_resident);
             }
         }
         if (!sync()) return;
@@ -828,11 +1047,11 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
 }
 
 // ------------------------------------------------------------------- host
-void mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::vector<MgChunk> &chunks,
-             int (&lchunk)[MG_MAXLEV + 2], int &lg, long long &nc) {
+bool mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::vector<MgChunk> &chunks,
+             int (&lchunk)[MG_MAXLEV + 2], int &lg, long long &nc, long long &npw, long long &ndinv) {
     const int nd = (int)doms.size();
     mgd.assign(nd, MgDom{});
-    nc = 0;
+    nc = npw = ndinv = 0;
     lg = 0;
     for (int d = 0; d < nd; ++d) {
         const DomainDesc &D = doms[d];
@@ -845,7 +1064,10 @@ void mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::
         int L = 0;
         g.m[0] = m;
         g.n[0] = n;
-        while ((m >= 3 || n >= 3) && L + 1 < MG_MAXLEV) {
+        while ((m >= 3 || n >= 3) && (long long)m * n > MG_DENSE_PTS) {
+            if (L + 1 >= MG_MAXLEV) return false;
+            g.pwo[L] = npw;
+            npw += (long long)m * n;
             g.hx[L] = m >= 3;
             g.hy[L] = n >= 3;
             m = g.hx[L] ? m / 2 : m;
@@ -857,6 +1079,8 @@ void mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::
             nc += (long long)m * n;
         }
         g.nlev = L + 1;
+        g.dio = ndinv;
+        ndinv += (long long)(m * n) * (m * n);
         // the block levels: the coarsest ones that fit MG_SMEM_PTS together
         long long tail = 0;
         g.lc = g.nlev;
@@ -883,6 +1107,7 @@ void mg_plan(const std::vector<DomainDesc> &doms, std::vector<MgDom> &mgd, std::
         }
     }
     lchunk[MG_MAXLEV + 1] = (int)chunks.size();
+    return true;
 }
 
 cudaError_t configure_mg(LaunchCfg &L, int device) {

@@ -92,6 +92,14 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// L2 prefetch of the box a load at the same coordinates would copy: no shared
+// memory and no mbarrier, only the DRAM reads of a later chunk started early.
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap *map, int x, int y, int z) {
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];\n" ::"l"(map), "r"(x),
+                 "r"(y), "r"(z)
+                 : "memory");
+}
+
 // Box loads of one array for planes [k0, k0 + CHN) of the tile at (x0, y0).
 template <typename V, int CHN>
 __device__ __forceinline__ void tma_halo(V *dst, const CUtensorMap *map, int x0, int y0, int k0,
@@ -102,6 +110,13 @@ template <typename V, int CHN>
 __device__ __forceinline__ void tma_own(V *dst, const CUtensorMap *map, int x0, int y0, int k0,
                                         uint64_t *bar) {
     tma_load_3d(dst, map, x0, y0, k0, bar);
+}
+template <typename V>
+__device__ __forceinline__ void tma_halo_prefetch(const CUtensorMap *map, int x0, int y0, int k0) {
+    tma_prefetch_3d(map, x0 - Halo<V>::XOFF, y0 - 1, k0);
+}
+__device__ __forceinline__ void tma_own_prefetch(const CUtensorMap *map, int x0, int y0, int k0) {
+    tma_prefetch_3d(map, x0, y0, k0);
 }
 // bytes of a halo box of CHN planes for a tile tx wide and ty high
 template <typename V, int CHN>

@@ -478,12 +478,18 @@ struct StageSize {
 // first.  A buffer is refilled with chunk st + STAGES once all threads are done
 // with it; when the tile is done, issue_next() starts the block's next tile so
 // its first chunks stream in during this tile's epilogue.
-template <int CHN, bool NEXT, typename Issue, typename PlaneFn, typename NextFn>
+// pf(st) starts the L2 prefetch of chunk st (PF_DIST chunks beyond the last
+// one issued into shared memory), so that more DRAM reads are in flight than
+// the staging buffers hold.
+template <int CHN, bool NEXT, typename Issue, typename PlaneFn, typename NextFn, typename Prefetch>
 __device__ __forceinline__ void march(int nz, StageBars &sb, bool prefetched, Issue issue, PlaneFn plane,
-                                      NextFn issue_next) {
+                                      NextFn issue_next, Prefetch pf) {
     const int nst = (nz + CHN - 1) / CHN;
     if (threadIdx.x == 0 && !prefetched)
         for (int q = 0; q < STAGES && q < nst; ++q) issue(q, q);
+    if constexpr (PF_DIST > 0)
+        if (threadIdx.x == 0)
+            for (int q = STAGES; q < STAGES + PF_DIST && q < nst; ++q) pf(q);
     bool next_ready = false;
     for (int st = 0; st < nst; ++st) {
         const int b = st % STAGES;
@@ -499,7 +505,11 @@ __device__ __forceinline__ void march(int nz, StageBars &sb, bool prefetched, Is
             plane(b, pl, k);
         }
         __syncthreads();
-        if (threadIdx.x == 0 && st + STAGES < nst) issue(st + STAGES, b);
+        if (threadIdx.x == 0 && st + STAGES < nst) {
+            issue(st + STAGES, b);
+            if constexpr (PF_DIST > 0)
+                if (st + STAGES + PF_DIST < nst) pf(st + STAGES + PF_DIST);
+        }
     }
     if (threadIdx.x == 0) issue_next();
 }
@@ -659,6 +669,23 @@ __device__ __forceinline__ void issue_C(const DevPtrs &P, int tile, int st, int 
     if (!first) tma_own<T, CHN>((T *)(B + 4 * HS + 3 * OB), maps + MAP_DD_O, td.x0, td.y0, k0, sb.bar + b);
 }
 
+// The L2 prefetch of the inner sweep's chunk st (the arrays issue_C loads).
+template <typename T>
+__device__ __forceinline__ void prefetch_C(const DevPtrs &P, int tile, int st, bool first, bool keep_p, int prev) {
+    constexpr int CHN = Chunk<T>::inner;
+    const TileDesc td = P.tiles[tile];
+    const CUtensorMap *maps = P.tmaps + (size_t)td.dom * NMAP;
+    const int k0 = st * CHN;
+    tma_halo_prefetch<T>(maps + (prev ? MAP_Z1_H : MAP_Z0_H), td.x0, td.y0, k0);
+    if (!first) tma_halo_prefetch<T>(maps + (prev ? MAP_T1_H : MAP_T0_H), td.x0, td.y0, k0);
+    if (!first || keep_p) tma_halo_prefetch<T>(maps + (prev ? MAP_P1_H : MAP_P0_H), td.x0, td.y0, k0);
+    tma_halo_prefetch<T>(maps + MAP_K_H, td.x0, td.y0, k0);
+    tma_own_prefetch(maps + MAP_D_O, td.x0, td.y0, k0);
+    tma_own_prefetch(maps + MAP_INV_O, td.x0, td.y0, k0);
+    tma_own_prefetch(maps + MAP_C_O, td.x0, td.y0, k0);
+    if (!first) tma_own_prefetch(maps + MAP_DD_O, td.x0, td.y0, k0);
+}
+
 // Issues chunks 0 and 1 of a tile (the prefetch of the block's next tile).
 template <int CHN, typename Issue>
 __device__ __forceinline__ void issue_head(int nz, Issue issue) {
@@ -750,7 +777,7 @@ __device__ __forceinline__ void phase_R(const DevPtrs &P, int tile, int tile_nex
         x_up = xc;
         K_up = Kc;
     };
-    march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next);
+    march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next, [](int) {});
     v[2] = (double)a2;
     if (cr.valid) back_sweep<T, DSMEM>(cr, s_d, fc, z);
 }
@@ -878,7 +905,8 @@ __device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_nex
             fd = fu;
             g += sxy;
         };
-        march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next);
+        march<CHN, true>(nz, sb, prefetched, issue, plane, issue_next,
+                         [&](int st) { prefetch_C<T>(P, tile, st, first, keep_p, prev); });
     };
     if (!first) sweep(SweepMode<2>{});
     else if (keep_p) sweep(SweepMode<1>{});
