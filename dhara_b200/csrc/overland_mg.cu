@@ -383,6 +383,52 @@ __device__ void galerkin_point(const DevPtrs &P, const DomainDesc &D, long long 
     for (int k = 0; k < 5; ++k) P.mg_a[(size_t)k * P.mg_nc + at] = acc[k];
 }
 
+// The restriction with the pre-smoothing folded in: V(1,1) starts from x = 0,
+// so level l's pre-smoothed x_l = W_l^-1 b_l and the coarse right-hand side
+// b_{l+1} = P^T (b_l - A_l x_l) = P^T (I - A_l W_l^-1) b_l, a fixed 5 x 5
+// stencil on b_l per coarse point (I, J), stored component-major in mg_r.
+// Its fine block starts at (2I - 1, 2J - 1) along a halved dimension and at
+// (I - 2, J - 2) along one that is not; entries outside the level are 0.
+__device__ __forceinline__ int rblock0(int I, bool halves) { return halves ? 2 * I - 1 : I - 2; }
+
+__device__ void restriction_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l,
+                                  int I, int J) {
+    const Lvl f = level(g, l), c = level(g, l + 1);
+    const bool hx = g.hx[l], hy = g.hy[l];
+    const int ox = rblock0(I, hx), oy = rblock0(J, hy);
+    double R[25];
+#pragma unroll
+    for (int k = 0; k < 25; ++k) R[k] = 0.0;
+    for (int b = 0; b < 3; ++b) {
+        int fy;
+        double vy;
+        child(J, b, hy, f.n, fy, vy);
+        if (vy == 0.0) continue;
+        for (int a = 0; a < 3; ++a) {
+            int fx;
+            double vx;
+            child(I, a, hx, f.m, fx, vx);
+            if (vx == 0.0) continue;
+            const double pf = slot(pw_at(P, g, l, fx, fy), child_slot(a, hx) + 2 * child_slot(b, hy));
+            if (pf == 0.0) continue;
+            R[(fy - oy) * 5 + (fx - ox)] += pf;
+            const Row9 r = row_of(P, D, ctot, g, l, f, fx, fy);
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const double av = r.a[dy + 1][dx + 1];
+                    if (av == 0.0) continue;
+                    const int gx = fx + dx, gy = fy + dy;
+                    const double wg = l == 0 ? 0.8 / olf_coef(P, D, f.at(gx, gy), ctot).dg
+                                             : __ldcg(P.mg_w + f.at(gx, gy));
+                    R[(gy - oy) * 5 + (gx - ox)] -= (pf * av) * wg;
+                }
+        }
+    }
+    const long long at = c.at(I, J);
+#pragma unroll
+    for (int k = 0; k < 25; ++k) P.mg_r[(size_t)k * P.mg_nc + at] = R[k];
+}
+
 // Smoother weight (levels >= 1) and interpolation weights of level l's point.
 __device__ __forceinline__ void weight_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g,
                                              int l, int i, int j) {
@@ -411,32 +457,26 @@ __device__ __forceinline__ double prolong_at(const MgDom &g, int l, const Lvl &c
 }
 
 // Grid levels (one barrier per level each way): level l+1 point (I, J) gets
-// b = P^T (b_l - A_l x_l) with the residual formed at its children, and
-// x = W^-1 b.  A child outside the level (weight 0) is read at a clamped
-// position, so the nine children's loads do not wait on branches.
+// b = P^T (I - A_l W_l^-1) b_l from its stored 5 x 5 stencil, and x = W^-1 b.
+// Positions outside the level (coefficient 0) are read clamped, so the 25
+// loads of b do not wait on branches.
 template <bool FINE>
 __device__ void restrict_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int I,
                                int J) {
     const Lvl f = level(g, l), c = level(g, l + 1);
     const LvlVec vf = vectors(P, l);
-    const bool hx = g.hx[l], hy = g.hy[l];
+    const int ox = rblock0(I, g.hx[l]), oy = rblock0(J, g.hy[l]);
+    const long long at = c.at(I, J);
+    const double *R = P.mg_r + at;
+    const size_t nc = (size_t)P.mg_nc;
     double acc = 0.0;
 #pragma unroll
-    for (int b = 0; b < 3; ++b)
+    for (int v = 0; v < 5; ++v) {
+        const int fy = clampi(oy + v, f.n);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            int fx, fy;
-            double vx, vy;
-            child(I, a, hx, f.m, fx, vx);
-            child(J, b, hy, f.n, fy, vy);
-            fx = clampi(fx, f.m);
-            fy = clampi(fy, f.n);
-            const float4 wv = pw_at(P, g, l, fx, fy);
-            const double pf = (vx != 0.0 && vy != 0.0) ? slot(wv, child_slot(a, hx) + 2 * child_slot(b, hy)) : 0.0;
-            const Row9 r = row_nb<FINE>(P, D, ctot, f, fx, fy);
-            acc += pf * (__ldcg(vf.b + f.at(fx, fy)) - apply_nb<FINE>(r, vf.x, f, fx, fy));
-        }
-    const long long at = c.at(I, J);
+        for (int u = 0; u < 5; ++u)
+            acc += __ldcg(R + (size_t)(v * 5 + u) * nc) * __ldcg(vf.b + f.at(clampi(ox + u, f.m), fy));
+    }
     P.mg_b[at] = acc;
     P.mg_x[at] = __ldcg(P.mg_w + at) * acc;
 }
@@ -870,12 +910,16 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
         }
     });
     if (!sync()) return;
-    // ---- set-up of the grid levels: A_l, then level l's smoother and
-    // interpolation weights where level l is a grid level
+    // ---- set-up of the grid levels: A_l and the restriction into level l,
+    // then level l's smoother and interpolation weights where level l is a
+    // grid level
     for (int l = 1; l <= Lg; ++l) {
         chunks(l, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
             int I, J;
-            if (point_of(ch, g, I, J)) galerkin_point(P, D, ctot, g, l - 1, I, J);
+            if (point_of(ch, g, I, J)) {
+                galerkin_point(P, D, ctot, g, l - 1, I, J);
+                restriction_point(P, D, ctot, g, l - 1, I, J);
+            }
         });
         if (!sync()) return;
         if (l < Lg) {
