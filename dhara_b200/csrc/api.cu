@@ -731,6 +731,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     rc |= dalloc(h, &d_mgc, std::max<size_t>(mgc.size(), 1));
     rc |= dalloc(h, &P.mg_a, 5 * (size_t)std::max(mg_nc, 1LL));
     for (double **q : {&P.mg_w, &P.mg_b, &P.mg_x, &P.mg_t}) rc |= dalloc(h, q, (size_t)std::max(mg_nc, 1LL));
+    rc |= dalloc(h, &P.mg_w0, C);
     rc |= dalloc(h, &P.mg_pw, (size_t)std::max(mg_npw, 1LL));
     rc |= dalloc(h, &P.mg_r, 25 * (size_t)std::max(mg_nc, 1LL));
     rc |= dalloc(h, &P.mg_dinv, (size_t)std::max(mg_ndinv, 1LL));
@@ -807,6 +808,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     e = e ? e : zero(P.mg_part, 5 * (size_t)std::max(nchunk0, 1) * 8);
     for (double *q : {P.mg_a, P.mg_w, P.mg_b, P.mg_x, P.mg_t})
         e = e ? e : zero(q, (q == P.mg_a ? 5 : 1) * (size_t)std::max(mg_nc, 1LL) * 8);
+    e = e ? e : zero(P.mg_w0, C * 8);
     e = e ? e : zero(P.mg_pw, (size_t)std::max(mg_npw, 1LL) * sizeof(float4));
     e = e ? e : zero(P.mg_r, 25 * (size_t)std::max(mg_nc, 1LL) * 8);
     e = e ? e : zero(P.mg_dinv, (size_t)std::max(mg_ndinv, 1LL) * 8);

@@ -260,6 +260,7 @@ struct DevPtrs {
     long long mg_nc;     // coarse points of all domains and levels
     double *mg_a;        // [5][mg_nc]: C, E, N, NE, NW of every coarse row
     double *mg_w, *mg_b, *mg_x, *mg_t;  // [mg_nc] 1/smoother weight, rhs, pre- and post-smoothed
+    double *mg_w0;       // [C] level 0's smoother weights 0.8 / a_ii (surface indexing)
     float4 *mg_pw;       // interpolation weights of every fine point to its (up to) four parents
     double *mg_r;        // [25][mg_nc] restriction stencils P^T (I - A W^-1) of the grid levels' coarse points
     double *mg_dinv;     // the coarsest level's inverse of every domain (row-major, symmetric)

@@ -370,19 +370,6 @@ __device__ __forceinline__ void galerkin_row(RowF rowf, WF wf, int fm, int fn, b
 }
 
 // ------------------------------------------------- grid-phase point kernels
-// Galerkin row (I, J) of level l+1 from level l in global memory.
-__device__ void galerkin_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l,
-                               int I, int J) {
-    const Lvl f = level(g, l), c = level(g, l + 1);
-    double acc[5];
-    galerkin_row([&](int i, int j) { return row_of(P, D, ctot, g, l, f, i, j); },
-                 [&](int i, int j) { return pw_at(P, g, l, i, j); }, f.m, f.n, g.hx[l], g.hy[l], c.m, c.n, I, J,
-                 acc);
-    const long long at = c.at(I, J);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) P.mg_a[(size_t)k * P.mg_nc + at] = acc[k];
-}
-
 // The restriction with the pre-smoothing folded in: V(1,1) starts from x = 0,
 // so level l's pre-smoothed x_l = W_l^-1 b_l and the coarse right-hand side
 // b_{l+1} = P^T (b_l - A_l x_l) = P^T (I - A_l W_l^-1) b_l, a fixed 5 x 5
@@ -391,40 +378,67 @@ __device__ void galerkin_point(const DevPtrs &P, const DomainDesc &D, long long 
 // (I - 2, J - 2) along one that is not; entries outside the level are 0.
 __device__ __forceinline__ int rblock0(int I, bool halves) { return halves ? 2 * I - 1 : I - 2; }
 
-__device__ void restriction_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l,
-                                  int I, int J) {
+// Set-up of coarse point (I, J) of level l+1 from level l in global memory:
+// its Galerkin row (C, E, N, NE, NW of P^T A_l P) and its restriction
+// stencil.  Every loop is unrolled and every load is at a position clamped
+// into the level, the terms outside it multiplied by zero, so the loads of a
+// child's row, its neighbours' weights and smoother weights are all in
+// flight together.  FINE: level 0 (5-point rows, smoother weights from
+// mg_w0).
+template <bool FINE>
+__device__ __noinline__ void setup_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int I,
+                            int J) {
     const Lvl f = level(g, l), c = level(g, l + 1);
     const bool hx = g.hx[l], hy = g.hy[l];
-    const int ox = rblock0(I, hx), oy = rblock0(J, hy);
-    double R[25];
+    const double *wsm = FINE ? P.mg_w0 : P.mg_w;
+    double R[25], acc[5];
 #pragma unroll
     for (int k = 0; k < 25; ++k) R[k] = 0.0;
-    for (int b = 0; b < 3; ++b) {
-        int fy;
-        double vy;
-        child(J, b, hy, f.n, fy, vy);
-        if (vy == 0.0) continue;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) acc[k] = 0.0;
+#pragma unroll 1
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
-            int fx;
-            double vx;
+            int fx, fy;
+            double vx, vy;
             child(I, a, hx, f.m, fx, vx);
-            if (vx == 0.0) continue;
-            const double pf = slot(pw_at(P, g, l, fx, fy), child_slot(a, hx) + 2 * child_slot(b, hy));
-            if (pf == 0.0) continue;
-            R[(fy - oy) * 5 + (fx - ox)] += pf;
-            const Row9 r = row_of(P, D, ctot, g, l, f, fx, fy);
+            child(J, b, hy, f.n, fy, vy);
+            fx = clampi(fx, f.m);
+            fy = clampi(fy, f.n);
+            const Row9 r = row_nb<FINE>(P, D, ctot, f, fx, fy);
+            const double pf =
+                (vx != 0.0 && vy != 0.0) ? slot(pw_at(P, g, l, fx, fy), child_slot(a, hx) + 2 * child_slot(b, hy)) : 0.0;
+            R[(b + 1) * 5 + (a + 1)] += pf;
+#pragma unroll
             for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
                 for (int dx = -1; dx <= 1; ++dx) {
-                    const double av = r.a[dy + 1][dx + 1];
-                    if (av == 0.0) continue;
-                    const int gx = fx + dx, gy = fy + dy;
-                    const double wg = l == 0 ? 0.8 / olf_coef(P, D, f.at(gx, gy), ctot).dg
-                                             : __ldcg(P.mg_w + f.at(gx, gy));
-                    R[(gy - oy) * 5 + (gx - ox)] -= (pf * av) * wg;
+                    if (FINE && dx != 0 && dy != 0) continue;  // compile-time: no corners at level 0
+                    const int gx = clampi(fx + dx, f.m), gy = clampi(fy + dy, f.n);
+                    const double av = pf * r.a[dy + 1][dx + 1];  // 0 outside the level or the child set
+                    R[(b + 1 + dy) * 5 + (a + 1 + dx)] -= av * __ldcg(wsm + f.at(gx, gy));
+                    const float4 wq = pw_at(P, g, l, gx, gy);
+                    int px0, px1, py0, py1;
+                    double ux0, ux1, uy0, uy1;
+                    parents2(gx, hx, c.m, px0, ux0, px1, ux1);
+                    parents2(gy, hy, c.n, py0, uy0, py1, uy1);
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) {
+                        const double u = ((s & 1) ? ux1 : ux0) * ((s & 2) ? uy1 : uy0);
+                        const double v = u != 0.0 ? av * slot(wq, s) : 0.0;
+                        const int di = ((s & 1) ? px1 : px0) - I, dj = ((s & 2) ? py1 : py0) - J;
+                        acc[0] += (di == 0 && dj == 0) ? v : 0.0;
+                        acc[1] += (di == 1 && dj == 0) ? v : 0.0;
+                        acc[2] += (di == 0 && dj == 1) ? v : 0.0;
+                        acc[3] += (di == 1 && dj == 1) ? v : 0.0;
+                        acc[4] += (di == -1 && dj == 1) ? v : 0.0;
+                    }
                 }
         }
-    }
     const long long at = c.at(I, J);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) P.mg_a[(size_t)k * P.mg_nc + at] = acc[k];
 #pragma unroll
     for (int k = 0; k < 25; ++k) P.mg_r[(size_t)k * P.mg_nc + at] = R[k];
 }
@@ -838,7 +852,7 @@ __device__ __forceinline__ DomSums decision_sums(const DevPtrs &P, const MgDom &
 }  // namespace
 
 // --------------------------------------------------------------- the solve
-__global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long ctot) {
+__global__ void __launch_bounds__(OLF_THREADS, 2) k_olf_mgcg(DevPtrs P, long long ctot) {
     extern __shared__ double s_mg[];  // a domain's block levels (block_vcycle)
     __shared__ int s_resident;        // the domain whose block levels are set up in s_mg
     const int tid = threadIdx.x;
@@ -897,8 +911,10 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
             const OlfCoef cf = olf_coef(P, D, c, ctot);
             const double b = P.olf_b[c];
             const double r = b - olf_av<false>(cf, P.H, c, f.nx, P.H[c]);
+            const double w0 = 0.8 / cf.dg;
+            P.mg_w0[c] = w0;
             P.olf_r[c] = r;
-            P.olf_z[c] = 0.8 / cf.dg * r;
+            P.olf_z[c] = w0 * r;
             v[0] += r * r;
             v[1] += b * b;
             if (g.lc >= 1) weight_point(P, D, ctot, g, 0, i, j);
@@ -917,8 +933,8 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
         chunks(l, [&](int, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
             int I, J;
             if (point_of(ch, g, I, J)) {
-                galerkin_point(P, D, ctot, g, l - 1, I, J);
-                restriction_point(P, D, ctot, g, l - 1, I, J);
+                if (l == 1) setup_point<true>(P, D, ctot, g, 0, I, J);
+                else setup_point<false>(P, D, ctot, g, l - 1, I, J);
             }
         });
         if (!sync()) return;
@@ -1075,11 +1091,10 @@ __global__ void __launch_bounds__(OLF_THREADS) k_olf_mgcg(DevPtrs P, long long c
                 double rr[1] = {0.0};
                 points0(ch, g, [&](int i, int j) {
                     const long long c = level(g, 0).at(i, j);
-                    const OlfCoef cf = olf_coef(P, D, c, ctot);
                     P.H[c] += alpha * P.olf_p[c];
                     const double r = P.olf_r[c] - alpha * P.olf_s[c];
                     P.olf_r[c] = r;
-                    P.olf_z[c] = 0.8 / cf.dg * r;
+                    P.olf_z[c] = __ldcg(P.mg_w0 + c) * r;
                     rr[0] += r * r;
                 });
                 olf_block_sum<1>(rr);
