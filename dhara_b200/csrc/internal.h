@@ -171,7 +171,9 @@ struct OlfSegState {
 // their operators (5), smoother weights, vectors b, x, t and interpolation
 // weights (4 floats) per point, and the coarsest level's inverse
 #define MG_SMEM_BYTES ((MG_SMEM_PTS * 11 + MG_DENSE_PTS * MG_DENSE_PTS) * 8)
+#ifndef MG_CHUNK0
 #define MG_CHUNK0 (4 * OLF_THREADS)  // points of a level-0 chunk (the CG's vectors), four per thread
+#endif
 struct MgDom {
     int nlev;                      // levels; 0 when the domain has no interior cell
     int lc;                        // first level run by the domain's block (levels lc .. nlev-1)
