@@ -417,7 +417,10 @@ int encode_map(CUtensorMap *m, const void *array, size_t elt, const DomainDesc &
     void *base = (void *)((const char *)array + (size_t)D.off3 * elt);
     if (((uintptr_t)base & 15) != 0 || (strides[0] & 15) != 0)
         return fail(DHARA_ERR_INVALID, "internal: unaligned 3D array for TMA");
-    CUresult r = enc(m, elt == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base,
+    const CUtensorMapDataType dt = elt == 2   ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                   : elt == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                              : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    CUresult r = enc(m, dt, 3, base,
                      dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(DHARA_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -442,8 +445,8 @@ int build_tensor_maps(dhara_handle *h) {
         rc |= encode_map(m + MAP_K_H, P.K, sT, D, true, chi);
         rc |= encode_map(m + MAP_D_O, P.D, sT, D, false, chi);
         rc |= encode_map(m + MAP_DD_O, P.d, sT, D, false, chi);
-        rc |= encode_map(m + MAP_INV_O, P.finv, sT, D, false, chi);
-        rc |= encode_map(m + MAP_C_O, P.fc, sT, D, false, chi);
+        rc |= encode_map(m + MAP_INV_O, P.finv, FACTOR_BYTES(h->mixed), D, false, chi);
+        rc |= encode_map(m + MAP_C_O, P.fc, FACTOR_BYTES(h->mixed), D, false, chi);
         rc |= encode_map(m + MAP_X64_H, P.x, 8, D, true, CH_R);
         rc |= encode_map(m + MAP_K64_H, P.K64, 8, D, true, CH_R);
         rc |= encode_map(m + MAP_D64_O, P.D64, 8, D, false, CH_R);
@@ -641,7 +644,7 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
         D.picard_maxiter = p.picard_maxiter; D.krylov_maxiter = p.krylov_maxiter;
         D.overland_maxiter = p.overland_maxiter;
         D.inner_maxiter = h->mixed ? (p.inner_maxiter > 0 ? p.inner_maxiter : p.krylov_maxiter) : p.krylov_maxiter;
-        D.nxp = (p.nx + 3) & ~3;
+        D.nxp = (p.nx + 7) & ~7;  // rows of every array 16-byte aligned, 2-byte factors included
         h->Ntot = (h->Ntot + 31) & ~31LL;  // 128-byte aligned base for FP32 and FP64
         D.off3 = h->Ntot; D.off2 = h->Ctot; D.offWE = h->WEtot; D.offSN = h->SNtot;
         h->Ntot += (long long)D.nxp * p.ny * p.nz;
@@ -703,8 +706,10 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     TileDesc *d_tiles = nullptr;
     rc |= dalloc(h, &d_tiles, h->tiles_cap);
     for (double **q : {&P.psin, &P.thetan, &P.psim, &P.x, &P.b, &P.ksat}) rc |= dalloc(h, q, N);
-    for (void **q : {&P.K, &P.D, &P.p0, &P.p1, &P.z0, &P.z1, &P.t0, &P.t1, &P.d, &P.finv, &P.fc})
+    for (void **q : {&P.K, &P.D, &P.p0, &P.p1, &P.z0, &P.z1, &P.t0, &P.t1, &P.d})
         rc |= dalloc_void(h, q, N * sT);
+    const size_t sF = FACTOR_BYTES(h->mixed);
+    for (void **q : {&P.finv, &P.fc}) rc |= dalloc_void(h, q, N * sF);
     if (h->mixed) {
         rc |= dalloc(h, &P.K64, N);
         rc |= dalloc(h, &P.D64, N);
@@ -793,7 +798,8 @@ int dhara_create(const dhara_params *params, int ndomains, int device, dhara_han
     auto zero = [&](void *p, size_t bytes) { return cudaMemsetAsync(p, 0, bytes, h->stream); };
     cudaError_t e = cudaSuccess;
     for (double *q : {P.psin, P.thetan, P.psim, P.x, P.b, P.ksat}) e = e ? e : zero(q, N * 8);
-    for (void *q : {P.K, P.D, P.p0, P.p1, P.z0, P.z1, P.t0, P.t1, P.d, P.finv, P.fc}) e = e ? e : zero(q, N * sT);
+    for (void *q : {P.K, P.D, P.p0, P.p1, P.z0, P.z1, P.t0, P.t1, P.d}) e = e ? e : zero(q, N * sT);
+    for (void *q : {P.finv, P.fc}) e = e ? e : zero(q, N * sF);
     for (double *q : {P.K64, P.D64}) e = e ? e : zero(q, N * 8);
     for (double *q : {P.ztopo, P.mann, P.h, P.H, P.ph, P.ppt, P.esoil, P.tr, P.hpoten, P.qtop, P.ktop, P.bcqb,
                       P.olf_b, P.olf_r, P.olf_p0, P.olf_p1, P.olf_z, P.olf_w, P.olf_s, P.olf_p})
@@ -1379,7 +1385,7 @@ int dhara_get_launch_count(dhara_handle *h, int64_t *count) {
 int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations) {
     if (!h) return fail(DHARA_ERR_INVALID, "NULL handle");
     if (set_dev(h)) return DHARA_ERR_CUDA;
-    const double sT = h->mixed ? 4.0 : 8.0;
+    const double sT = h->mixed ? 4.0 : 8.0, sF = (double)FACTOR_BYTES(h->mixed);
     double total = 0.0;
     int64_t iters = 0;
     for (int d = 0; d < h->ndom; ++d) {
@@ -1391,14 +1397,15 @@ int dhara_get_krylov_traffic(dhara_handle *h, double *bytes, int64_t *iterations
         const double solves = (double)dg.picard_iters_total;
         const double cycles = (double)dg.refine_iters_total;
         const double upd = cycles > solves ? cycles - solves : 0.0;
-        // inner iteration (one sweep): reads the previous z, t, p and K, D,
-        // 1/den, c', d and writes z, t, p, d (12 T-words; the back sweep's second
-        // read of c' follows the staged read and is not counted); the first
-        // sweep of a cycle reads no previous t, p or d (3 words fewer).  Outer
-        // residual R: x, b, K64, D64 (f64) + writes z and the two factors (3 T)
-        // + c' read back (1 T); update U: x read+write (f64) + d, p (2 T).
-        total += N * (12.0 * sT * (double)dg.krylov_iters_total - 3.0 * sT * upd +
-                      (32.0 + 4.0 * sT) * cycles + (16.0 + 2.0 * sT) * upd);
+        // inner iteration (one sweep): reads the previous z, t, p and K, D, d
+        // and the factors 1/den, c', and writes z, t, p, d (10 T-words and 2
+        // factors; the back sweep's second read of c' follows the staged read
+        // and is not counted); the first sweep of a cycle reads no previous t,
+        // p or d (3 T-words fewer).  Outer residual R: x, b, K64, D64 (f64) +
+        // writes z (T) and the two factors + c' read back; update U: x
+        // read+write (f64) + d, p (2 T).
+        total += N * ((10.0 * sT + 2.0 * sF) * (double)dg.krylov_iters_total - 3.0 * sT * upd +
+                      (32.0 + sT + 3.0 * sF) * cycles + (16.0 + 2.0 * sT) * upd);
         iters += dg.krylov_iters_total;
     }
     if (bytes) *bytes = total;

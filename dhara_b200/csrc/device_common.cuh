@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <type_traits>
+#include <cuda_bf16.h>
 
 #include "internal.h"
 

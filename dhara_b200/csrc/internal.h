@@ -36,6 +36,16 @@
 #ifndef STAGES
 #define STAGES 2
 #endif
+// storage of the column preconditioner's factors 1/den and c': narrower than
+// the inner precision (bf16 in mixed mode, FP32 in FP64 mode) when set
+#ifndef FACTOR_NARROW_F32
+#define FACTOR_NARROW_F32 0
+#endif
+#ifndef FACTOR_NARROW_F64
+#define FACTOR_NARROW_F64 1
+#endif
+// bytes of one stored factor
+#define FACTOR_BYTES(mixed) ((mixed) ? (FACTOR_NARROW_F32 ? 2 : 4) : (FACTOR_NARROW_F64 ? 4 : 8))
 // inner sweep: chunks prefetched into L2 beyond the staged ones (0: none).
 // Measured per FP32 / FP64 inner iteration on the 512x512x40 storm: 0 chunks
 // 0.1681 / 0.2595 ms, 1 chunk 0.1644 / 0.2548, 2 chunks 0.1664 / 0.2609,

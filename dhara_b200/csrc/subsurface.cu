@@ -457,13 +457,48 @@ struct Chunk {
     static constexpr int inner = sizeof(T) == 4 ? CHUNK_F32 : CHUNK_F64;
 };
 
+// Storage type of the column preconditioner's factors 1/den and c': bf16 in
+// mixed mode with FACTOR_NARROW_F32, FP32 in FP64 mode with FACTOR_NARROW_F64.  Any rounding of
+// the stored pair still defines a symmetric positive definite M = L D L^T
+// (D = 1/inv > 0, L from c'), and every use of M -- phase R's z = M^-1 r,
+// the sweep's forward and back substitutions and its z.M z -- goes through
+// the stored values, so the inner CG sees one fixed preconditioner.
+template <typename T>
+struct Fac {
+    using type = T;
+};
+#if FACTOR_NARROW_F32
+template <>
+struct Fac<float> {
+    using type = __nv_bfloat16;
+};
+#endif
+#if FACTOR_NARROW_F64
+template <>
+struct Fac<double> {
+    using type = float;
+};
+#endif
+template <typename T, typename F>
+__device__ __forceinline__ T fac_get(F v) {
+    if constexpr (std::is_same<F, __nv_bfloat16>::value) return (T)__bfloat162float(v);
+    else return (T)v;
+}
+template <typename F, typename T>
+__device__ __forceinline__ F fac_put(T v) {
+    if constexpr (std::is_same<F, __nv_bfloat16>::value) return __float2bfloat16_rn((float)v);
+    else return (F)v;
+}
+
 // Bytes of one staging buffer of each phase (the kernel reserves STAGES buffers
 // of the largest).
 template <typename T>
 struct StageSize {
     static constexpr int C = Chunk<T>::inner;
+    using F = typename Fac<T>::type;
     // inner sweep: z, t, p of the previous iteration and K (halo); D, 1/den, c', d (own)
-    static constexpr size_t I = 4 * (size_t)halo_slot<T, C>() + 4 * (size_t)own_bytes<T, C>();
+    static constexpr size_t I =
+        4 * (size_t)halo_slot<T, C>() + 2 * (size_t)own_bytes<T, C>() + 2 * (size_t)own_bytes<F, C>();
     // phase R: x, K64 (halo); D64, b (own), all FP64
     static constexpr size_t R = 2 * (size_t)halo_slot<double, CH_R>() + 2 * (size_t)own_bytes<double, CH_R>();
     static constexpr size_t buffer() { return I > R ? I : R; }
@@ -542,8 +577,8 @@ __device__ __forceinline__ void put_dprime(T dp, T *s_d, int k, T *__restrict__ 
 #ifndef BACK_BATCH
 #define BACK_BATCH 4
 #endif
-template <typename T, bool DSMEM>
-__device__ __forceinline__ void back_sweep(const ColumnRef &cr, const T *s_d, const T *__restrict__ fc,
+template <typename T, bool DSMEM, typename F>
+__device__ __forceinline__ void back_sweep(const ColumnRef &cr, const T *s_d, const F *__restrict__ fc,
                                            T *__restrict__ z) {
     T zn = T(0);
     const unsigned g0 = (unsigned)cr.g0, sxy = (unsigned)cr.sxy;
@@ -554,7 +589,7 @@ __device__ __forceinline__ void back_sweep(const ColumnRef &cr, const T *s_d, co
             const int k = k0 - q;
             if (k >= 0) {
                 const unsigned g = g0 + (unsigned)k * sxy;
-                cl[q] = fc[g];
+                cl[q] = fac_get<T>(fc[g]);
                 dl[q] = DSMEM ? s_d[k * TILE_THREADS + threadIdx.x] : z[g];
             }
         }
@@ -576,6 +611,15 @@ template <>
 __device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
 template <>
 __device__ __forceinline__ double recip(double x) { return 1.0 / x; }
+
+// a / b where the quotient only feeds a sum of positive terms (z.M z): the
+// hardware reciprocal's approximation (about 2 ulp) in FP32
+template <typename T>
+__device__ __forceinline__ T quot(T a, T b);
+template <>
+__device__ __forceinline__ float quot(float a, float b) { return __fdividef(a, b); }
+template <>
+__device__ __forceinline__ double quot(double a, double b) { return a / b; }
 
 // Face masks of a column: 1 where the face is interior, 0 on a domain face.
 struct Masks {
@@ -648,8 +692,9 @@ template <typename T>
 __device__ __forceinline__ void issue_C(const DevPtrs &P, int tile, int st, int b, unsigned char *stage,
                                         StageBars &sb, bool first, bool keep_p, int prev) {
     constexpr int CHN = Chunk<T>::inner;
-    constexpr unsigned HS = halo_slot<T, CHN>(), OB = own_bytes<T, CHN>();
-    static_assert(HS % 128 == 0 && OB % 128 == 0, "TMA destinations must be 128-byte aligned");
+    using F = typename Fac<T>::type;
+    constexpr unsigned HS = halo_slot<T, CHN>(), OB = own_bytes<T, CHN>(), OF = own_bytes<F, CHN>();
+    static_assert(HS % 128 == 0 && OB % 128 == 0 && OF % 128 == 0, "TMA destinations must be 128-byte aligned");
     const TileDesc td = P.tiles[tile];
     const DomainDesc &D = P.dom[td.dom];
     const unsigned HB = halo_bytes<T, CHN>(D.tx, D.ty);
@@ -658,15 +703,15 @@ __device__ __forceinline__ void issue_C(const DevPtrs &P, int tile, int st, int 
     const int k0 = st * CHN;
     const bool with_p = !first || keep_p;
     sb.issued(b);
-    mbar_expect_tx(sb.bar + b, (first ? 2 : 3) * HB + (with_p ? HB : 0) + (first ? 3 : 4) * OB);
+    mbar_expect_tx(sb.bar + b, (first ? 2 : 3) * HB + (with_p ? HB : 0) + (first ? 1 : 2) * OB + 2 * OF);
     tma_halo<T, CHN>((T *)B, maps + (prev ? MAP_Z1_H : MAP_Z0_H), td.x0, td.y0, k0, sb.bar + b);
     if (!first) tma_halo<T, CHN>((T *)(B + HS), maps + (prev ? MAP_T1_H : MAP_T0_H), td.x0, td.y0, k0, sb.bar + b);
     if (with_p) tma_halo<T, CHN>((T *)(B + 2 * HS), maps + (prev ? MAP_P1_H : MAP_P0_H), td.x0, td.y0, k0, sb.bar + b);
     tma_halo<T, CHN>((T *)(B + 3 * HS), maps + MAP_K_H, td.x0, td.y0, k0, sb.bar + b);
     tma_own<T, CHN>((T *)(B + 4 * HS), maps + MAP_D_O, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<T, CHN>((T *)(B + 4 * HS + OB), maps + MAP_INV_O, td.x0, td.y0, k0, sb.bar + b);
-    tma_own<T, CHN>((T *)(B + 4 * HS + 2 * OB), maps + MAP_C_O, td.x0, td.y0, k0, sb.bar + b);
-    if (!first) tma_own<T, CHN>((T *)(B + 4 * HS + 3 * OB), maps + MAP_DD_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<F, CHN>((F *)(B + 4 * HS + OB), maps + MAP_INV_O, td.x0, td.y0, k0, sb.bar + b);
+    tma_own<F, CHN>((F *)(B + 4 * HS + OB + OF), maps + MAP_C_O, td.x0, td.y0, k0, sb.bar + b);
+    if (!first) tma_own<T, CHN>((T *)(B + 4 * HS + OB + 2 * OF), maps + MAP_DD_O, td.x0, td.y0, k0, sb.bar + b);
 }
 
 // The L2 prefetch of the inner sweep's chunk st (the arrays issue_C loads).
@@ -709,8 +754,9 @@ __device__ __forceinline__ void phase_R(const DevPtrs &P, int tile, int tile_nex
     // z goes into the buffer that holds the last iteration's p (the next
     // sweep reads both from there)
     T *__restrict__ z = (T *)(ldcg(&P.kctrl[P.tiles[tile].dom].parity) ? P.z1 : P.z0);
-    T *__restrict__ finv = (T *)P.finv;
-    T *__restrict__ fc = (T *)P.fc;
+    using F = typename Fac<T>::type;
+    F *__restrict__ finv = (F *)P.finv;
+    F *__restrict__ fc = (F *)P.fc;
     const size_t BUF = StageSize<T>::buffer();
     auto buf = [&](int b) { return stage + b * BUF; };
     auto issue = [&](int st, int b) { issue_R<T>(P, tile, st, b, stage, sb); };
@@ -763,12 +809,15 @@ __device__ __forceinline__ void phase_R(const DevPtrs &P, int tile, int tile_nex
         const T fu = k + 1 < nz ? f.z * (Kt + (T)K_dn) : T(0);
         const T bd = (lateral_diag((T)Dk, fw, fe, fs, fn) + fd) + fu;
         const T den = bd + fd * cprev;  // b_k - a_k c'_{k-1} with a_k = -fd
-        const T inv = fixed ? T(0) : recip(den);
-        const T cp = -fu * inv;
+        // the stored (rounded) factors are the ones applied, here as in the sweeps
+        const F inv_s = fac_put<F>(fixed ? T(0) : recip(den));
+        const T inv = fac_get<T>(inv_s);
+        const F cp_s = fac_put<F>(-fu * inv);
+        const T cp = fac_get<T>(cp_s);
         const T y = rT - cprev * yprev;
         const T dp = y * inv;
-        finv[g] = inv;
-        fc[g] = cp;
+        finv[g] = inv_s;
+        fc[g] = cp_s;
         put_dprime<T, DSMEM>(dp, s_d, k, z + g);
         a2 += y * dp;
         cprev = cp;
@@ -808,12 +857,13 @@ __device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_nex
     // the tile shape is a compile-time constant of each instantiation
     const Halo<T> H(TXC, TXC == 32 ? 5 : 4, TILE_THREADS / TXC);
     constexpr unsigned HB = halo_slot<T, CHN>();
-    constexpr int S = CHN * OWN_PLANE;
     T *__restrict__ z_out = (T *)(prev ? P.z0 : P.z1);
     T *__restrict__ p_out = (T *)(prev ? P.p0 : P.p1);
     T *__restrict__ t_out = (T *)(prev ? P.t0 : P.t1);
     T *__restrict__ d = (T *)P.d;
-    const T *__restrict__ fc = (const T *)P.fc;
+    using F = typename Fac<T>::type;
+    constexpr unsigned OB = own_bytes<T, CHN>(), OF = own_bytes<F, CHN>();
+    const F *__restrict__ fc = (const F *)P.fc;
     const size_t BUF = StageSize<T>::buffer();
     auto buf = [&](int b) { return stage + b * BUF; };
     auto issue = [&](int st, int b) { issue_C<T>(P, tile, st, b, stage, sb, first, keep_p, prev); };
@@ -826,8 +876,8 @@ __device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_nex
     const int nz = cr.nz, hc = H.hc, oc = threadIdx.x;
     const FaceW<T> f = face_weights(cr, w);
     // carried down the column: this plane's z, p, K and upper face coefficient,
-    // the plane above's z and p, the forward sweep's c'_{k-1} and y_{k-1}
-    T zc = T(0), pc = T(0), Kc = T(0), fd = T(0), z_up = T(0), p_up = T(0), cprev = T(0), yprev = T(0);
+    // the plane above's p, the forward sweep's c'_{k-1} and y_{k-1}
+    T zc = T(0), pc = T(0), Kc = T(0), fd = T(0), p_up = T(0), cprev = T(0), yprev = T(0);
     T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
     // 32-bit cell offsets (a handle holds fewer than 2^31 cells): fewer live
     // registers in the sweep than 64-bit indices
@@ -849,13 +899,17 @@ __device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_nex
             const T *st = (const T *)(buf(b) + HB) + pl * H.plane;
             const T *sp = (const T *)(buf(b) + 2 * HB) + pl * H.plane;
             const T *sK = (const T *)(buf(b) + 3 * HB) + pl * H.plane;
-            const T *own = (const T *)(buf(b) + 4 * HB) + pl * OWN_PLANE + oc;
+            const unsigned char *ob = buf(b) + 4 * HB;
+            const T *ownD = (const T *)ob + pl * OWN_PLANE + oc;
+            const F *ownI = (const F *)(ob + OB) + pl * OWN_PLANE + oc;
+            const F *ownC = (const F *)(ob + OB + OF) + pl * OWN_PLANE + oc;
+            const T *ownd = (const T *)(ob + OB + 2 * OF) + pl * OWN_PLANE + oc;
             if (k == 0) {
                 zc = zv(sz, st, hc);
                 pc = pz(zc, sp, hc);
                 Kc = sK[hc];
             }
-            const T Dk = own[0], inv = own[S], cp = own[2 * S];
+            const T Dk = ownD[0], inv = fac_get<T>(ownI[0]), cp = fac_get<T>(ownC[0]);
             T z_dn = T(0), p_dn = T(0), K_dn = T(0), fu = T(0);
             if (k + 1 < nz) {
                 const T *nzz = sz + H.plane, *ntt = st + H.plane, *npp = sp + H.plane, *nK = sK + H.plane;
@@ -878,27 +932,25 @@ __device__ __forceinline__ void phase_C(const DevPtrs &P, int tile, int tile_nex
             const bool fixed = Dk < T(0);  // Dirichlet cell: identity row, z = p = 0 there
             T q = Dk * pc + (fw * (pc - pw) + fe * (pc - pe)) + (fs * (pc - ps) + fn * (pc - pn)) +
                   (fd * (pc - p_up) + fu * (pc - p_dn));
-            // (M z)_k with M the column's tridiagonal part of A
-            T Mz = lateral_diag(Dk, fw, fe, fs, fn) * zc + (fd * (zc - z_up) + fu * (zc - z_dn));
-            if (fixed) {
-                q = T(0);
-                Mz = T(0);
-            }
+            // z.M z with M = L D L^T from the stored factors: the column's sum of
+            // (z_k + c'_k z_{k+1})^2 / inv_k (0 on a fixed cell, where inv = 0)
+            const T u = zc + cp * z_dn;
+            const T zMz = fixed ? T(0) : quot(u * u, inv);
+            if (fixed) q = T(0);
             a0 += pc * q;
             a1 += zc * q;
-            a3 += zc * Mz;
+            a3 += zMz;
             const T y = q - cprev * yprev;
             const T dp = y * inv;
             a2 += y * dp;
             z_out[g] = zc;
             p_out[g] = pc;
-            if constexpr (MODE == 2) d[g] = own[3 * S] + ap * sp[hc];
+            if constexpr (MODE == 2) d[g] = ownd[0] + ap * sp[hc];
             else d[g] = T(0);
             put_dprime<T, DSMEM>(dp, s_d, k, t_out + g);
             cprev = cp;
             yprev = y;
             p_up = pc;
-            z_up = zc;
             zc = z_dn;
             pc = p_dn;
             Kc = K_dn;
