@@ -438,13 +438,17 @@ __global__ void __launch_bounds__(TILE_THREADS) k_dir_rows(DevPtrs P) {
 // and after the barrier alpha_i = rho_i / sigma and
 //   rho_{i+1} = rho_i - 2 alpha_i mu + alpha_i^2 nu    (r_i.t_i = z_i.q by
 //   symmetry of M), beta_{i+1} = rho_{i+1} / rho_i.
-// rho_i is evaluated directly from z_i (M z is column-local) rather than
-// carried by the update formula, which would accumulate cancellation; the
-// formula is only ever applied to a freshly computed rho.  x's last update
-// (alpha of the final iteration times its p) is applied in U.
+// rho_i is evaluated directly from z_i rather than carried by the update
+// formula, which would accumulate cancellation; the formula is only ever
+// applied to a freshly computed rho.  With M = L D L^T from the stored
+// factors, z.M z = sum_k (z_k + c'_k z_{k+1})^2 / inv_k per column: a sum of
+// positive terms (forming M z from the operator's coefficients instead
+// cancels, and costs the FP32 solve 3 % more inner iterations on the
+// 512x512x40 storm).  x's last update (alpha of the final iteration times its
+// p) is applied in U.
 // Per inner iteration each cell reads z, t, p, K (at the halo), D, 1/den, c',
-// d and writes z, t, p, d: 12 words, against 15 and two grid barriers for the
-// textbook two-phase iteration.
+// d and writes z, t, p, d: 12 words (the two factors FP32 in FP64 mode),
+// against 15 and two grid barriers for the textbook two-phase iteration.
 
 template <typename T>
 struct StencilW {
