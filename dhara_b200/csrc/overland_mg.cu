@@ -46,10 +46,12 @@
 // in one block out of shared memory with block barriers, their operators set
 // up there and kept for the whole solve when the block owns one domain; the
 // finer ones run as grid phases, level 0 in chunks of MG_CHUNK0 points (four
-// per thread) and the others one point per thread.  The residual is fused
-// into the restriction and the prolongation into the post-smoothing (each
-// point recomputes the few neighbour values it needs), so a grid level costs
-// one barrier on the way down and one on the way up; with q = A z + beta q
+// per thread) and the others one point per thread.  The pre-smoothing and
+// the residual are folded into a stored 5 x 5 restriction stencil per coarse
+// point (P^T (I - A W^-1), formed at set-up), and the prolongation is fused
+// into the post-smoothing (each point recomputes the few neighbour values it
+// needs), so a grid level costs one barrier on the way down and one on the
+// way up; with q = A z + beta q
 // the CG forms p and q in one phase.  An iteration with L grid levels is
 // 2 L + 3 barriers (eleven on a 512 x 512 surface).  Every reduction runs over
 // chunks in a fixed order, so results do not depend on the block count.
