@@ -1059,19 +1059,33 @@ __global__ void __launch_bounds__(OLF_THREADS, 2) k_olf_mgcg(DevPtrs P, long lon
                     chunk_sums<2>(P, g, slots, v);
                     beta = it == 0 ? 0.0 : v[0] / v[1];
                 }
+                // every point's loads first, then the stores (the compiler may
+                // not move a point's loads across an earlier point's stores)
+                constexpr int NQ = MG_CHUNK0 / OLF_THREADS;
+                const Lvl f = level(g, 0);
+                long long cq[NQ];
+                double zq[NQ], azq[NQ], pq0[NQ], sq0[NQ];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const int o = tid + q * OLF_THREADS;
+                    const int pt = ch.first + (o < ch.count ? o : 0);
+                    cq[q] = f.at(pt % f.m, pt / f.m);
+                    const OlfCoef cf = olf_coef(P, D, cq[q], ctot);
+                    zq[q] = __ldcg(P.olf_w + cq[q]);
+                    azq[q] = olf_av<true>(cf, P.olf_w, cq[q], f.nx, zq[q]);
+                    pq0[q] = it == 0 ? 0.0 : __ldcg(P.olf_p + cq[q]);
+                    sq0[q] = it == 0 ? 0.0 : __ldcg(P.olf_s + cq[q]);
+                }
                 double pq[1] = {0.0};
-                points0(ch, g, [&](int i, int j) {
-                    const Lvl f = level(g, 0);
-                    const long long c = f.at(i, j);
-                    const OlfCoef cf = olf_coef(P, D, c, ctot);
-                    const double z = __ldcg(P.olf_w + c);
-                    const double az = olf_av<true>(cf, P.olf_w, c, f.nx, z);
-                    const double p = it == 0 ? z : z + beta * P.olf_p[c];
-                    const double q = it == 0 ? az : az + beta * P.olf_s[c];
-                    P.olf_p[c] = p;
-                    P.olf_s[c] = q;
-                    pq[0] += p * q;
-                });
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    if (tid + q * OLF_THREADS >= ch.count) continue;
+                    const double p = it == 0 ? zq[q] : zq[q] + beta * pq0[q];
+                    const double qv = it == 0 ? azq[q] : azq[q] + beta * sq0[q];
+                    P.olf_p[cq[q]] = p;
+                    P.olf_s[cq[q]] = qv;
+                    pq[0] += p * qv;
+                }
                 olf_block_sum<1>(pq);
                 if (tid == 0) pslot(MP_PQ, k) = pq[0];
             });
@@ -1090,15 +1104,31 @@ __global__ void __launch_bounds__(OLF_THREADS, 2) k_olf_mgcg(DevPtrs P, long lon
                     chunk_sums<2>(P, g, slots, v);
                     alpha = (v[1] > 0.0 && v[0] > 0.0 && v[1] < 1e300) ? v[0] / v[1] : 0.0;
                 }
+                constexpr int NQ = MG_CHUNK0 / OLF_THREADS;
+                const Lvl f = level(g, 0);
+                long long cq[NQ];
+                double hq[NQ], pq[NQ], rq[NQ], sq[NQ], wq[NQ];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const int o = tid + q * OLF_THREADS;
+                    const int pt = ch.first + (o < ch.count ? o : 0);
+                    cq[q] = f.at(pt % f.m, pt / f.m);
+                    hq[q] = __ldcg(P.H + cq[q]);
+                    pq[q] = __ldcg(P.olf_p + cq[q]);
+                    rq[q] = __ldcg(P.olf_r + cq[q]);
+                    sq[q] = __ldcg(P.olf_s + cq[q]);
+                    wq[q] = __ldcg(P.mg_w0 + cq[q]);
+                }
                 double rr[1] = {0.0};
-                points0(ch, g, [&](int i, int j) {
-                    const long long c = level(g, 0).at(i, j);
-                    P.H[c] += alpha * P.olf_p[c];
-                    const double r = P.olf_r[c] - alpha * P.olf_s[c];
-                    P.olf_r[c] = r;
-                    P.olf_z[c] = __ldcg(P.mg_w0 + c) * r;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    if (tid + q * OLF_THREADS >= ch.count) continue;
+                    P.H[cq[q]] = hq[q] + alpha * pq[q];
+                    const double r = rq[q] - alpha * sq[q];
+                    P.olf_r[cq[q]] = r;
+                    P.olf_z[cq[q]] = wq[q] * r;
                     rr[0] += r * r;
-                });
+                }
                 olf_block_sum<1>(rr);
                 if (tid == 0) pslot(MP_RR, k) = rr[0];
             });
