@@ -501,8 +501,8 @@ __device__ void restrict_point(const DevPtrs &P, const DomainDesc &D, long long 
 // with x' = x_l + P t_{l+1} formed at the point and its neighbours (clamped
 // positions where a neighbour is outside the level, whose coefficient is 0).
 template <bool FINE>
-__device__ void smooth_up_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int i,
-                                int j) {
+__device__ __forceinline__ double smooth_up_value(const DevPtrs &P, const DomainDesc &D, long long ctot,
+                                                  const MgDom &g, int l, int i, int j) {
     const Lvl f = level(g, l), c = level(g, l + 1);
     const LvlVec vf = vectors(P, l);
     const Row9 r = row_nb<FINE>(P, D, ctot, f, i, j);
@@ -520,7 +520,13 @@ __device__ void smooth_up_point(const DevPtrs &P, const DomainDesc &D, long long
         }
     const long long at = f.at(i, j);
     const double winv = FINE ? 0.8 / r.a[1][1] : __ldcg(P.mg_w + at);
-    vf.t[at] = xc + winv * (__ldcg(vf.b + at) - ax);
+    return xc + winv * (__ldcg(vf.b + at) - ax);
+}
+
+template <bool FINE>
+__device__ void smooth_up_point(const DevPtrs &P, const DomainDesc &D, long long ctot, const MgDom &g, int l, int i,
+                                int j) {
+    vectors(P, l).t[level(g, l).at(i, j)] = smooth_up_value<FINE>(P, D, ctot, g, l, i, j);
 }
 
 // ----------------------------------------------------------- block levels
@@ -1036,12 +1042,27 @@ __global__ void __launch_bounds__(OLF_THREADS, 2) k_olf_mgcg(DevPtrs P, long lon
         // ---- level 0: z (the preconditioned residual, in olf_w) and r.z
         chunks(0, [&](int k, const MgChunk &ch, const MgDom &g, const DomainDesc &D) {
             if (!active(ch.dom)) return;
+            // every point's value first, then the stores (as in X and Y)
+            constexpr int NQ = MG_CHUNK0 / OLF_THREADS;
+            const Lvl f = level(g, 0);
+            long long cq[NQ];
+            double tq[NQ], rq[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const int o = tid + q * OLF_THREADS;
+                const int pt = ch.first + (o < ch.count ? o : 0);
+                const int i = pt % f.m, j = pt / f.m;
+                cq[q] = f.at(i, j);
+                tq[q] = g.lc > 0 ? smooth_up_value<true>(P, D, ctot, g, 0, i, j) : __ldcg(P.olf_w + cq[q]);
+                rq[q] = __ldcg(P.olf_r + cq[q]);
+            }
             double v[1] = {0.0};
-            points0(ch, g, [&](int i, int j) {
-                if (g.lc > 0) smooth_up_point<true>(P, D, ctot, g, 0, i, j);
-                const long long c = level(g, 0).at(i, j);
-                v[0] += __ldcg(P.olf_r + c) * __ldcg(P.olf_w + c);
-            });
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                if (tid + q * OLF_THREADS >= ch.count) continue;
+                if (g.lc > 0) P.olf_w[cq[q]] = tq[q];
+                v[0] += rq[q] * tq[q];
+            }
             olf_block_sum<1>(v);
             if (tid == 0) pslot(MP_RZ + (it & 1), k) = v[0];
         });
